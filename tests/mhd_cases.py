@@ -1,0 +1,310 @@
+"""Shared test helpers: seeded initial states and ctypes bindings for the two
+CPU checkers (the oracle restatement in oracle/ and, when it was built, the
+reference's own code in oracle/_ref).  Test infrastructure only.
+
+Arrays are padded SoA storage, shape (ny + 2g, nx + 2g) in C order, so that
+flat index (i + g) + (nx + 2g) * (j + g) matches core/grid.hpp:158-161 of the
+reference.  Component order: rho, mx, my, mz, energy, bx_face, by_face,
+bz_cell.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "libquasar_mhd_oracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libquasar_mhd_ref.so")
+
+COMPONENTS = ("rho", "mx", "my", "mz", "energy", "bx_face", "by_face", "bz_cell")
+PERIODIC = (0, 0, 0, 0)
+OUTFLOW = (1, 1, 1, 1)
+
+
+def nghost(order: int) -> int:
+    return 4 if order == 7 else 3 if order == 5 else 2
+
+
+# --------------------------------------------------------------------------
+# Initial states (primitive profiles -> conserved, face-sampled B).
+# --------------------------------------------------------------------------
+def _centres(n, ng, length, origin=0.0):
+    i = np.arange(-ng, n + ng, dtype=np.float64)
+    d = length / n
+    return (i + 0.5) * d + origin
+
+
+def _assemble(rho, vx, vy, vz, p, bx, by, bz, gamma):
+    kin = 0.5 * rho * (vx * vx + vy * vy + vz * vz)
+    mag = 0.5 * (bx * bx + by * by + bz * bz)
+    energy = p / (gamma - 1.0) + kin + mag
+    return [np.ascontiguousarray(a, dtype=np.float64) for a in
+            (rho, rho * vx, rho * vy, rho * vz, energy, bx, by, bz)]
+
+
+def orszag_tang(n, order=5, gamma=5.0 / 3.0, amplitude=1.0, ny=None):
+    """Orszag-Tang on [0,1]^2: rho=25/(36 pi), p=5/(12 pi),
+    v=(-sin 2 pi y, sin 2 pi x), face B = B0 (-sin 2 pi y, sin 4 pi x),
+    B0 = 1/sqrt(4 pi).  `amplitude` scales rho, p by a and B by sqrt(a)."""
+    ny = n if ny is None else ny
+    ng = nghost(order)
+    x = _centres(n, ng, 1.0)
+    y = _centres(ny, ng, 1.0)
+    X, Y = np.meshgrid(x, y, indexing="xy")
+    pi = math.pi
+    a = amplitude
+    rho = np.full_like(X, a * 25.0 / (36.0 * pi))
+    p = np.full_like(X, a * 5.0 / (12.0 * pi))
+    b0 = math.sqrt(a) / math.sqrt(4.0 * pi)
+    vx = -np.sin(2 * pi * Y)
+    vy = np.sin(2 * pi * X)
+    bx = -b0 * np.sin(2 * pi * Y)
+    by = b0 * np.sin(4 * pi * X)
+    z = np.zeros_like(X)
+    return _assemble(rho, vx, vy, z, p, bx, by, z, gamma)
+
+
+def rotor(n, order=7, gamma=5.0 / 3.0):
+    """MHD rotor on [0,1]^2: rho=10 inside r<0.1, linear taper to 1 at
+    r=0.115, angular velocity 20 inside (u0=2, r0=0.1), p=1, Bx=5/sqrt(4 pi)."""
+    ng = nghost(order)
+    x = _centres(n, ng, 1.0)
+    X, Y = np.meshgrid(x, x, indexing="xy")
+    rx, ry = X - 0.5, Y - 0.5
+    r = np.hypot(rx, ry)
+    r0, r1, u0 = 0.1, 0.115, 2.0
+    f = np.clip((r1 - r) / (r1 - r0), 0.0, 1.0)
+    f = np.where(r <= r0, 1.0, np.where(r >= r1, 0.0, f))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sf = np.where(r <= r0, u0 / r0, np.where(r < r1, f * u0 / np.maximum(r, 1e-300), 0.0))
+    rho = 1.0 + f * (10.0 - 1.0)
+    vx, vy = -sf * ry, sf * rx
+    p = np.ones_like(X)
+    z = np.zeros_like(X)
+    bx = np.full_like(X, 5.0 / math.sqrt(4.0 * math.pi))
+    return _assemble(rho, vx, vy, z, p, bx, z, z, gamma)
+
+
+def blast(n, order=7, gamma=5.0 / 3.0):
+    """MHD blast on [0,1]^2: p=100 for r<0.1 else 0.1, rho=1,
+    Bx=By=10/sqrt(8 pi)."""
+    ng = nghost(order)
+    x = _centres(n, ng, 1.0)
+    X, Y = np.meshgrid(x, x, indexing="xy")
+    r = np.hypot(X - 0.5, Y - 0.5)
+    p = np.where(r < 0.1, 100.0, 0.1)
+    rho = np.ones_like(X)
+    b = 10.0 / math.sqrt(8.0 * math.pi)
+    z = np.zeros_like(X)
+    return _assemble(rho, z, z, z, p, np.full_like(X, b), np.full_like(X, b), z, gamma)
+
+
+# --------------------------------------------------------------------------
+# ctypes bindings
+# --------------------------------------------------------------------------
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _ptrs(arrs):
+    return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+class _Lib:
+    prefix = ""
+
+    def __init__(self, path):
+        self.lib = ctypes.CDLL(path)
+        p = self.prefix
+        L = self.lib
+        getattr(L, p + "last_error").restype = ctypes.c_char_p
+        for f in ("seed", "read"):
+            getattr(L, p + f).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+        getattr(L, p + "cfl").argtypes = [ctypes.c_void_p, _dp]
+        getattr(L, p + "step").argtypes = [ctypes.c_void_p, ctypes.c_double]
+        getattr(L, p + "destroy").argtypes = [ctypes.c_void_p]
+        getattr(L, p + "substeps").argtypes = [ctypes.c_void_p]
+        getattr(L, p + "hlld_flux_x").argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
+        getattr(L, p + "mp5").argtypes = [ctypes.c_void_p]
+        getattr(L, p + "mp5").restype = ctypes.c_double
+        getattr(L, p + "mp7").argtypes = [ctypes.c_void_p]
+        getattr(L, p + "mp7").restype = ctypes.c_double
+
+    def err(self):
+        return getattr(self.lib, self.prefix + "last_error")().decode()
+
+    def hlld_flux_x(self, left, right, gamma):
+        left = np.ascontiguousarray(left, dtype=np.float64)
+        right = np.ascontiguousarray(right, dtype=np.float64)
+        out = np.zeros(8)
+        getattr(self.lib, self.prefix + "hlld_flux_x")(left.ctypes.data, right.ctypes.data, gamma, out.ctypes.data)
+        return out
+
+    def mp(self, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        f = self.prefix + ("mp5" if v.size == 5 else "mp7")
+        return getattr(self.lib, f)(v.ctypes.data)
+
+
+class CpuSolver:
+    """Common driver over either checker: seed, cfl, step, read."""
+
+    def __init__(self, lib: _Lib, handle, nx, ny, order):
+        self.L = lib
+        self.h = handle
+        self.nx, self.ny, self.order = nx, ny, order
+        self.ng = nghost(order)
+        self.shape = (ny + 2 * self.ng, nx + 2 * self.ng)
+
+    def __del__(self):
+        try:
+            getattr(self.L.lib, self.L.prefix + "destroy")(self.h)
+        except Exception:
+            pass
+
+    def _call(self, name, *args):
+        rc = getattr(self.L.lib, self.L.prefix + name)(self.h, *args)
+        if rc != 0:
+            raise RuntimeError(self.L.err())
+
+    def seed(self, comps):
+        for c, a in enumerate(comps):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            assert a.shape == self.shape
+            self._call("seed", c, a.ctypes.data, a.size)
+
+    def read(self):
+        out = []
+        for c in range(8):
+            a = np.empty(self.shape)
+            self._call("read", c, a.ctypes.data, a.size)
+            out.append(a)
+        return out
+
+    def cfl(self):
+        d = ctypes.c_double()
+        self._call("cfl", ctypes.byref(d))
+        return d.value
+
+    def step(self, dt):
+        self._call("step", dt)
+
+    def substeps(self):
+        return getattr(self.L.lib, self.L.prefix + "substeps")(self.h)
+
+    def residual(self, comps):
+        """L(u) of an arbitrary padded state: dict of dudt, ifx, ify, fx, fy, ez."""
+        comps = [np.ascontiguousarray(a, dtype=np.float64) for a in comps]
+        mk = lambda k: [np.zeros(self.shape) for _ in range(k)]  # noqa: E731
+        out = dict(dudt=mk(8), ifx=mk(16), ify=mk(16), fx=mk(8), fy=mk(8),
+                   ez=np.zeros(self.shape), cell_ez=np.zeros(self.shape))
+        args = [_ptrs(comps), _ptrs(out["dudt"]), _ptrs(out["ifx"]), _ptrs(out["ify"]),
+                _ptrs(out["fx"]), _ptrs(out["fy"]), ctypes.c_void_p(out["ez"].ctypes.data),
+                ctypes.c_void_p(out["cell_ez"].ctypes.data)]
+        if isinstance(self.L, RefLib):
+            args += [None, None]
+        self._call("residual", *args)
+        return out
+
+
+class OracleLib(_Lib):
+    prefix = "qor_"
+
+    def __init__(self, path=ORACLE_SO):
+        super().__init__(path)
+        L = self.lib
+        L.qor_create.restype = ctypes.c_void_p
+        L.qor_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                 ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.qor_residual.argtypes = [ctypes.c_void_p] * 9
+        L.qor_count_flops.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
+
+    def solver(self, nx, ny, order, gamma=5.0 / 3.0, cfl=0.4, bc=PERIODIC, lx=1.0, ly=1.0, counting=False):
+        h = self.lib.qor_create(nx, ny, lx, ly, order, gamma, cfl, (ctypes.c_int * 4)(*bc), int(counting))
+        if not h:
+            raise RuntimeError(self.err())
+        return CpuSolver(self, h, nx, ny, order)
+
+    def count_flops(self, solver: CpuSolver, steps: int):
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        solver._call("count_flops", steps, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+
+class RefLib(_Lib):
+    prefix = "qref_"
+
+    def __init__(self, path=REF_SO):
+        super().__init__(path)
+        L = self.lib
+        L.qref_create.restype = ctypes.c_void_p
+        L.qref_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                  ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
+        L.qref_residual.argtypes = [ctypes.c_void_p] * 11
+        L.qref_divb.argtypes = [ctypes.c_void_p, _dp]
+
+    def solver(self, nx, ny, order, gamma=5.0 / 3.0, cfl=0.4, bc=PERIODIC, lx=1.0, ly=1.0):
+        h = self.lib.qref_create(nx, ny, lx, ly, 0.0, 0.0, order, gamma, cfl, (ctypes.c_int * 4)(*bc))
+        if not h:
+            raise RuntimeError(self.err())
+        return CpuSolver(self, h, nx, ny, order)
+
+
+def oracle_available():
+    return os.path.exists(ORACLE_SO)
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+# --------------------------------------------------------------------------
+# Metrics
+# --------------------------------------------------------------------------
+def interior(a, ng):
+    return a[ng:-ng, ng:-ng]
+
+
+def rel_l1(a, b, ng):
+    """Relative L1 over the interior: sum|a-b| / sum|b| (0 if both zero)."""
+    x, y = interior(a, ng), interior(b, ng)
+    den = np.abs(y).sum()
+    num = np.abs(x - y).sum()
+    return 0.0 if num == 0.0 else num / max(den, 1e-300)
+
+
+def _evolved(a, c, ng, nx, ny):
+    if c == 5:
+        return a[ng:ng + ny, ng:ng + nx + 1]
+    if c == 6:
+        return a[ng:ng + ny + 1, ng:ng + nx]
+    return a[ng:ng + ny, ng:ng + nx]
+
+
+# Relative L1 is taken per physical group so that a component which is zero
+# analytically (mz, bz in 2-D problems) is measured against its vector.
+GROUPS = ((0,), (1, 2, 3), (4,), (5, 6, 7))
+
+
+def state_rel_l1(sa, sb, ng, nx, ny):
+    """Max over groups (rho, momentum, energy, field) of
+    sum|a-b| / sum|b| on the evolved region (cells plus owned high faces)."""
+    worst = 0.0
+    for grp in GROUPS:
+        num = sum(np.abs(_evolved(sa[c], c, ng, nx, ny) - _evolved(sb[c], c, ng, nx, ny)).sum() for c in grp)
+        den = sum(np.abs(_evolved(sb[c], c, ng, nx, ny)).sum() for c in grp)
+        if num == 0.0:
+            continue
+        worst = max(worst, num / den if den > 0 else np.inf)
+    return worst
+
+
+def divb_max(s, ng, nx, ny, dx, dy):
+    bx, by = s[5], s[6]
+    d = ((bx[ng:ng + ny, ng + 1:ng + nx + 1] - bx[ng:ng + ny, ng:ng + nx]) / dx +
+         (by[ng + 1:ng + ny + 1, ng:ng + nx] - by[ng:ng + ny, ng:ng + nx]) / dy)
+    return float(np.abs(d).max())
