@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark: MHD zone-updates/s of the plain FP64 step on one B200.
+
+Workload (default): MHD rotor, 4096^2, MP7 + HLLD + upwind CT, SSP-RK3,
+outflow boundaries, gamma 5/3, CFL 0.4 (capped to 0.2 by the MP limiter as in
+the reference); seeded synthetic analytic initial state.  One step = one
+auto-dt SSP-RK3 step (cfl_limit + step), dt kept on the device.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--case rotor|blast]
+                    [--n 4096] [--impl b200|reference]
+
+N > 1 (torchrun, one process per GPU) runs N independent replicas (the
+single-instance step is not domain-decomposed here); the value is the sum over
+ranks with the time taken as the max over ranks.
+
+Printed JSON line: value = device-timed zone-updates/s with the state resident
+in HBM; e2e = the same metric through the public C ABI with host buffers
+(seed from pinned host memory, per-step cfl_limit read-back, final state read
+back); roofline = the reconstruction kernel (the largest share of the step)
+against the FP64 FMA peak measured on the same GPU; cpu_baseline = the
+reference's own MHD path built for the CPU, on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+WORLD = int(os.environ.get("WORLD_SIZE", "1"))
+RANK = int(os.environ.get("RANK", "0"))
+LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
+if WORLD > 1 and "CUDA_VISIBLE_DEVICES" not in os.environ:
+    # the solver library carries its own CUDA runtime: pin the device before
+    # any CUDA initialisation in this process
+    os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+PHASES = ["control", "reconstruction", "face_flux", "cell_emf", "corner_emf", "update",
+          "ghost_fill", "collocation"]
+# kernels per auto-dt step: step_begin, 2 reconstruct, 2 face_flux, cell_emf,
+# corner_emf, dt | stage 0 update, 2 ghost, colloc_check | 2 x (2 reconstruct,
+# 2 face_flux, cell_emf, corner_emf, update, 2 ghost, colloc_check) | step_end
+LAUNCHES_PER_STEP = 8 + 4 + 2 * 10 + 1
+FLOP_PHASE = {"reconstruction": "reconstruction", "face_flux": "face_flux", "cell_emf": "cell_emf",
+              "corner_emf": "corner_emf", "update": "update", "collocation": "collocation"}
+
+
+# ---------------------------------------------------------------------------
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--case", default="rotor", choices=["rotor", "blast"])
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--order", type=int, default=7, choices=[5, 7])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+class Dist:
+    """Barrier and max/sum over ranks (gloo on host scalars)."""
+
+    def __init__(self):
+        self.pg = None
+        if WORLD > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if WORLD > 1:
+            self.dist.barrier()
+
+    def reduce(self, x, op):
+        if WORLD == 1:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX if op == "max" else self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if WORLD > 1:
+            self.dist.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during a region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        dev = os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]
+        rows = [l.split(", ") for l in self.lines if l]
+        rows = [r for r in rows if len(r) >= 9 and (r[0] == dev or not dev.isdigit())]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows)}
+
+
+# ---------------------------------------------------------------------------
+def reference_cpu(case, order, steps, warmup, n=128):
+    """The reference's own MHD path built for the CPU (oracle/_ref), all host
+    threads, on an n^2 sample of the workload; falls back to the oracle port."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import mhd_cases as M
+    from quasar_b200 import ics
+    ic = ics.GENERATORS[case](n, order=order)
+    bc = (1, 1, 1, 1)
+    if M.ref_available():
+        lib, kind = M.RefLib(), "reference"
+    else:
+        lib, kind = M.OracleLib(), "port"
+    s = lib.solver(n, n, order, bc=bc)
+    s.seed(ic)
+    for _ in range(warmup):
+        s.step(s.cfl())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step(s.cfl())
+    wall = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": n * n * steps / wall, "unit": "zone-updates/s", "cores": cores, "kind": kind,
+            "sample": f"{case} {n}^2 MP{order} outflow, {warmup} untimed + {steps} timed steps "
+                      f"(cfl_limit + step_unchecked), {cores} OpenMP threads"}
+
+
+def run_reference_arm(a):
+    if RANK != 0:
+        return
+    steps, warmup = max(1, min(a.steps, 3)), max(0, min(a.warmup, 1))
+    cpu = reference_cpu(a.case, a.order, steps, warmup)
+    line = {"impl": "reference", "metric": "MHD zone-updates/s (plain FP64 step)",
+            "value": cpu["value"], "unit": "zone-updates/s", "n_gpus": a.gpus, "steps": steps,
+            "warmup": warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{a.case} MP{a.order}+HLLD+CT SSP-RK3 outflow", "n": a.n,
+                       "sample_n": 128},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def make_solver(a):
+    from quasar_b200 import mhd
+    cfg = mhd.MhdConfig()
+    cfg.grid = mhd.Grid2D(a.n, a.n, 1.0, 1.0)
+    cfg.reconstruction = "mp7" if a.order == 7 else "mp5"
+    cfg.boundary = mhd.MhdBoundarySpec(["outflow"] * 4, ["outflow"] * 4)
+    return mhd.MhdSolver2D(cfg)
+
+
+def seed(s, comps):
+    from quasar_b200.ics import COMPONENTS
+    for name, arr in zip(COMPONENTS, comps):
+        s.seed_state(name, arr)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+        return
+    import ctypes
+
+    from quasar_b200 import _native, ics
+    L = _native.lib()
+    dist = Dist()
+    comps = ics.GENERATORS[a.case](a.n, order=a.order)
+    s = make_solver(a)
+    seed(s, comps)
+    ms, done = ctypes.c_double(), ctypes.c_int()
+
+    def timed(k):
+        _native.check(L.qmhd_solver_time_auto_steps(s._h, k, ctypes.byref(ms), ctypes.byref(done)))
+        if done.value != k:
+            raise RuntimeError(f"device loop stopped after {done.value} of {k} steps")
+        return ms.value
+
+    timed(max(a.warmup, 3))
+    dist.barrier()
+    clocks = Clocks()
+    clocks.start()
+    t_ms = timed(a.steps)
+    clk = clocks.stop()
+    dist.barrier()
+    t_ms = dist.reduce(t_ms, "max")
+    zones = a.n * a.n
+    value = zones * a.steps * WORLD / (t_ms * 1e-3)
+
+    # per-phase device times of one step, for the roofline
+    ph = (ctypes.c_double * 8)()
+    _native.check(L.qmhd_solver_profile_step(s._h, ph, 8))
+    phase_ms = dict(zip(PHASES, list(ph)))
+    peak = ctypes.c_double()
+    _native.check(L.qmhd_fp64_fma_peak(ctypes.byref(peak)))
+    flops = {}
+    fpath = os.path.join(ROOT, "profiles", "flop_counts.json")
+    if os.path.exists(fpath):
+        table = json.load(open(fpath))["workloads"].get(f"{a.case}_mp{a.order}", {})
+        flops = table.get("per_zone_step", {})
+    dom = "reconstruction"
+    achieved = flops.get(dom, 0.0) * zones / (phase_ms[dom] * 1e-3) / 1e12 if phase_ms[dom] > 0 else None
+    step_flops = sum(flops.values()) if flops else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        tt = json.load(open(tpath)).get(f"{a.case}_mp{a.order}_reconstruction")
+        if tt:
+            traffic = tt["bytes_per_zone_step"] * zones
+    roofline = {"bound": "fp64", "kernel": "k_reconstruct (x and y, 3 stages)",
+                "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": (achieved / peak.value) if achieved else None, "traffic": traffic,
+                "peak_source": "FP64 FMA probe on this GPU (qmhd_fp64_fma_peak); "
+                               "MEASURED_PEAKS.json holds no FP64 figure",
+                "step_flop_per_zone": step_flops,
+                "step_achieved_tflops": (step_flops * value / WORLD / 1e12) if step_flops else None,
+                "phase_ms_per_step": {k: round(v, 4) for k, v in phase_ms.items()}}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not a.no_e2e:
+        import torch
+        pinned = []
+        for arr in comps:
+            t = torch.empty(arr.size, dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = arr.reshape(-1)
+            pinned.append(t)
+        out = [torch.empty(arr.size, dtype=torch.float64, pin_memory=True) for arr in comps]
+        s2 = make_solver(a)
+        names = ics.COMPONENTS
+        k_e2e = a.steps
+        dist.barrier()
+        t0 = time.perf_counter()
+        for name, t in zip(names, pinned):
+            _native.check(L.qmhd_solver_seed_state(s2._h, name.encode(), t.data_ptr(), t.numel()))
+        dt = ctypes.c_double()
+        for _ in range(k_e2e):
+            _native.check(L.qmhd_solver_cfl_limit(s2._h, ctypes.byref(dt)))
+            _native.check(L.qmhd_solver_step_unchecked(s2._h, dt.value))
+        for name, t in zip(names, out):
+            _native.check(L.qmhd_solver_state_component_to_host(s2._h, name.encode(), t.data_ptr(),
+                                                                t.numel()))
+        wall = time.perf_counter() - t0
+        wall = dist.reduce(wall, "max")
+        bytes_state = sum(arr.nbytes for arr in comps)
+        e2e = {"value": zones * k_e2e * WORLD / wall, "unit": "zone-updates/s",
+               "h2d_bytes_per_step": bytes_state / k_e2e,
+               "d2h_bytes_per_step": bytes_state / k_e2e + 8,
+               "how": "seed_state x8 from pinned host, per step cfl_limit (8-byte dt read back) + "
+                      "step_unchecked, state_component_to_host x8; host wall clock"}
+        del s2
+
+    cpu = None
+    if RANK == 0 and WORLD == 1 and not a.no_cpu:
+        cpu = reference_cpu(a.case, a.order, 3, 1)
+
+    if RANK == 0:
+        line = {"metric": "MHD zone-updates/s (plain FP64 step)", "value": value,
+                "unit": "zone-updates/s", "n_gpus": WORLD, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": t_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"{a.case} {a.n}^2 MP{a.order}+HLLD+upwind CT, SSP-RK3, "
+                                       "outflow, gamma 5/3, CFL 0.4 (0.2 effective)",
+                           "n": a.n, "order": a.order, "parallelism": f"replicas x{WORLD}",
+                           "l2": "state 1 GB+ per register, larger than L2"},
+                "gpu_launches": LAUNCHES_PER_STEP * a.steps,
+                "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

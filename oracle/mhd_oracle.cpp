@@ -99,6 +99,33 @@ class Solver {
 
   int order_now() const { return low_order > 0 ? low_order : cfg.order; }
 
+  // ---- FLOP attribution (counting instance only) --------------------------
+  // Phases: 0 collocation, 1 reconstruction, 2 face flux, 3 cell EMF,
+  // 4 corner EMF, 5 update (flux difference, curl, combine), 6 CFL rates,
+  // 7 admissibility, 8 work the reference repeats (not algorithmic).
+  std::uint64_t phase_flops[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  bool colloc_free = false;  // per-load collocation is charged once per cell instead
+  void charge(int p) {
+    if constexpr (!kPar) {
+      phase_flops[p] += flop_counter();
+      flop_counter() = 0;
+    }
+  }
+  void charge_collocation(const Field& u) {
+    if constexpr (!kPar) {
+      if (!colloc_free) return;
+      charge(8);
+      colloc_free = false;
+      for (int j = -g.ng; j < g.ny + g.ng; ++j)
+        for (int i = -g.ng; i < g.nx + g.ng; ++i) {
+          (void)face_to_cell(u.c[BX], 0, i, j, 0);
+          (void)face_to_cell(u.c[BY], 1, j, i, 0);
+        }
+      colloc_free = true;
+      charge(0);
+    }
+  }
+
   // ---- staggered-B collocation: mhd_staggering.hpp:42-50, 77-236 -------
   static int colloc_width(int extent, int ng) {
     const int req = ng >= 4 ? 8 : ng >= 3 ? 6 : ng >= 2 ? 4 : 2;
@@ -121,6 +148,17 @@ class Solver {
   }
   R face_to_cell(const std::vector<double>& f, int axis, int cell, int fixed,
                  int coll) const {
+    if constexpr (!kPar) {
+      if (colloc_free) {
+        const std::uint64_t saved = flop_counter();
+        auto* self = const_cast<Solver*>(this);
+        self->colloc_free = false;
+        const R r = face_to_cell(f, axis, cell, fixed, coll);
+        self->colloc_free = true;
+        flop_counter() = saved;
+        return r;
+      }
+    }
     const int n = axis == 0 ? g.nx : g.ny;
     const int lo = -g.ng, hi = n + g.ng - 1;
     if (coll == 1) {  // mhd_staggering.hpp:243-254
@@ -632,6 +670,14 @@ class Solver {
         const size_t k = g.idx(i, j);
         if (!((i == g.nx && !phx) || (j == g.ny && !phy)))
           cell_ez[k] = qval(cell_average_ez(u, i, j, order));
+      }
+    charge(3);
+    // Directional face EMFs: the reference re-solves every face problem here
+    // (mhd_ct.hip:330-359); the fluxes above already hold the same values.
+#pragma omp parallel for collapse(2) schedule(dynamic, 16) if (kPar)
+    for (int j = 0; j <= g.ny; ++j)
+      for (int i = 0; i <= g.nx; ++i) {
+        const size_t k = g.idx(i, j);
         if (j < g.ny || (j == g.ny && phy)) {
           xface_ez[k] = qval(-face_flux(ifx, 0, i, j, order, hll_only).by);
           xnj[k] = face_no_jump(ifx, 0, i, j, order) ? 1 : 0;
@@ -641,6 +687,7 @@ class Solver {
           ynj[k] = face_no_jump(ify, 1, i, j, order) ? 1 : 0;
         }
       }
+    charge(8);
 #pragma omp parallel for collapse(2) schedule(static) if (kPar)
     for (int j = 0; j <= g.ny; ++j)
       for (int i = 0; i <= g.nx; ++i) {
@@ -673,6 +720,7 @@ class Solver {
         else e = crsum3(ex, ey, -centered);
         ez[k] = qval(e);
       }
+    charge(4);
   }
   // mhd_ct.hip:893-931 (Cartesian)
   void curl_rate(Field& dudt) const {
@@ -699,16 +747,24 @@ class Solver {
       ensure_solenoidal();
       ensure_admissible(order <= 1 ? 1 : 0);
     }
+    charge(7);
     for (auto& c : dudt.c) std::fill(c.begin(), c.end(), 0.0);
+    if (!current) charge_collocation(u);
     if (!current) reconstruct(u, 0, order, ifx);
+    charge(1);
     face_fluxes(ifx, 0, order, flux_x);
+    charge(2);
     if (!current) reconstruct(u, 1, order, ify);
+    charge(1);
     face_fluxes(ify, 1, order, flux_y);
+    charge(2);
     iface_cache_valid = false;
     flux_difference(flux_x, 0, dudt);
     flux_difference(flux_y, 1, dudt);
+    charge(5);
     ct_emf(u, order);
     curl_rate(dudt);
+    charge(5);
   }
 
   // ---- SSP-RK3 combine: mhd_update.hip:113-206, mhd_solver.cpp:840-906 ---
@@ -891,8 +947,11 @@ class Solver {
     ensure_solenoidal();
     ensure_admissible(coll);
     const int order = coll > 0 ? 1 : cfg.order;
+    charge(7);
+    charge_collocation(rk[0]);
     reconstruct(rk[0], 0, order, ifx);
     reconstruct(rk[0], 1, order, ify);
+    charge(1);
     iface_cache_valid = true;
     iface_cache_src = &rk[0];
     iface_cache_order = order;
@@ -906,6 +965,7 @@ class Solver {
         local = std::isfinite(local) ? std::max(0.0, local) : std::numeric_limits<double>::infinity();
         maxrate = std::max(maxrate, local);
       }
+    charge(6);
     const double eff = order >= 5 ? std::min(cfg.cfl, 0.2) : cfg.cfl;
     if (!std::isfinite(maxrate))
       throw std::runtime_error("MhdSolver2D: non-finite state encountered in CFL reduction");
@@ -939,10 +999,13 @@ class Solver {
     else if (stage == 1) { out = &rk[2]; a = 3.0 / 4.0; b = 1.0 / 4.0; c = (1.0 / 4.0) * dt; }
     else { out = &rk[0]; a = 1.0 / 3.0; b = 2.0 / 3.0; c = (2.0 / 3.0) * dt; }
     const Field& us = stage == 2 ? rk[2] : rk[1];
+    charge(8);
     rk_stage(*out, rk[0], us, residual, a, b, c);
+    charge(5);
     fill_ghosts(*out);
     if (out == &rk[0]) iface_cache_valid = false;
     const double th = stage_theta(stage);
+    charge(7);
     if (!(th >= 1.0)) throw Retry{std::isfinite(th) ? th : 0.0};
   }
   void integrate(double dt) {  // ssprk_integrator.cpp:40-53
@@ -1050,6 +1113,8 @@ void seed_into(S* s, int comp, const double* d) {
 }  // namespace
 
 extern "C" {
+
+int qor_count_phases(void* p, int steps, double* out);
 
 const char* qor_last_error() { return g_err.c_str(); }
 
@@ -1170,10 +1235,12 @@ int qor_residual(void* p, const double* const* in8, double* const* dudt,
   }
 }
 
-// Algorithmic FLOPs (oracle_count.hpp rules) of `steps` full steps of the
-// counting instance, cfl_limit included, divided by nx*ny*steps.
-int qor_count_flops(void* p, int steps, double* flops_per_zone_step,
-                    double* flops_cfl, double* flops_stage) {
+// FLOPs (oracle_count.hpp rules) per zone-step of `steps` full steps of the
+// counting instance, cfl_limit included: *as_written counts every operation
+// the reference's code performs, *algorithmic applies the de-duplication
+// rules of qor_count_phases, *cfl is the CFL-rate share of the latter.
+int qor_count_flops(void* p, int steps, double* as_written, double* algorithmic,
+                    double* cfl) {
   auto* h = static_cast<Handle*>(p);
   Counting* s = h->c;
   if (!s) {
@@ -1181,20 +1248,59 @@ int qor_count_flops(void* p, int steps, double* flops_per_zone_step,
     return -1;
   }
   try {
-    std::uint64_t total = 0, cfl_total = 0;
+    for (auto& v : s->phase_flops) v = 0;
+    qoracle::flop_counter() = 0;
+    s->colloc_free = false;
     for (int k = 0; k < steps; ++k) {
-      qoracle::flop_counter() = 0;
       const double dt = s->cfl_limit();
-      cfl_total += qoracle::flop_counter();
-      total += qoracle::flop_counter();
-      qoracle::flop_counter() = 0;
+      s->charge(7);
       s->step_unchecked(dt);
-      total += qoracle::flop_counter();
+      s->charge(7);
     }
     const double zones = double(s->g.nx) * double(s->g.ny) * double(steps);
-    *flops_per_zone_step = double(total) / zones;
-    *flops_cfl = double(cfl_total) / zones;
-    *flops_stage = double(total - cfl_total) / zones / 3.0;
+    double total = 0;
+    for (auto v : s->phase_flops) total += double(v);
+    *as_written = total / zones;
+    double ph[8];
+    const int rc = qor_count_phases(p, steps, ph);
+    if (rc != 0) return rc;
+    double alg = 0;
+    for (double v : ph) alg += v;
+    *algorithmic = alg;
+    *cfl = ph[6];
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// Per-phase algorithmic FLOPs per zone-step (phases as Solver::charge):
+// collocation counted once per padded cell per stage (the reference repeats
+// it for every load), the face-EMF re-solve not counted (it repeats the flux
+// solve), and each CFL face rate once (the per-cell reduction evaluates every
+// interior face twice).  out[0..7].
+int qor_count_phases(void* p, int steps, double* out) {
+  auto* h = static_cast<Handle*>(p);
+  Counting* s = h->c;
+  if (!s) {
+    g_err = "qor_count_phases: not a counting instance";
+    return -1;
+  }
+  try {
+    s->colloc_free = true;
+    for (auto& v : s->phase_flops) v = 0;
+    qoracle::flop_counter() = 0;
+    for (int k = 0; k < steps; ++k) {
+      const double dt = s->cfl_limit();
+      s->charge(7);
+      s->step_unchecked(dt);
+      s->charge(7);
+    }
+    const double zones = double(s->g.nx) * double(s->g.ny) * double(steps);
+    for (int k = 0; k < 8; ++k) out[k] = double(s->phase_flops[k]) / zones;
+    out[6] *= 0.5;
+    s->colloc_free = false;
     return 0;
   } catch (const std::exception& e) {
     g_err = e.what();

@@ -1,0 +1,84 @@
+"""ctypes binding of the in-tree CUDA library (include/quasar_mhd.h).
+
+The library is required: there is no CPU fallback.  If it is missing, build
+it with `python -m quasar_b200.build`; if no CUDA device is present, solver
+construction fails with the CUDA error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libquasar_mhd_b200.so")
+
+QMHD_OK = 0
+QMHD_INVALID_ARGUMENT = -1
+QMHD_RUNTIME_ERROR = -2
+QMHD_DEVICE_ERROR = -3
+
+EXPORTS = (
+    "qmhd_last_error", "qmhd_solver_create", "qmhd_solver_destroy", "qmhd_solver_grid",
+    "qmhd_solver_storage_size", "qmhd_solver_seed_state", "qmhd_solver_state_component_to_host",
+    "qmhd_solver_cfl_limit", "qmhd_solver_step", "qmhd_solver_step_unchecked",
+    "qmhd_solver_advance", "qmhd_solver_divergence_b_max", "qmhd_solver_conserved_cell_totals",
+    "qmhd_solver_last_positivity_substeps", "qmhd_solver_advance_auto",
+)
+EXT_EXPORTS = ("qmhd_solver_time_auto_steps", "qmhd_solver_profile_step", "qmhd_fp64_fma_peak")
+
+
+class QmhdConfig(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+        ("origin_x", ctypes.c_double), ("origin_y", ctypes.c_double),
+        ("reconstruction_order", ctypes.c_int),
+        ("gamma", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("boundary", ctypes.c_int * 4),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"quasar_b200 CUDA library not found at {LIB_PATH}; build it with "
+            "`python -m quasar_b200.build` (there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    L.qmhd_last_error.restype = ctypes.c_char_p
+    L.qmhd_solver_create.argtypes = [ctypes.POINTER(QmhdConfig), ctypes.POINTER(vp)]
+    L.qmhd_solver_destroy.argtypes = [vp]
+    L.qmhd_solver_destroy.restype = None
+    L.qmhd_solver_grid.argtypes = [vp, ip, ip, ip]
+    L.qmhd_solver_storage_size.argtypes = [vp]
+    L.qmhd_solver_storage_size.restype = ctypes.c_longlong
+    L.qmhd_solver_seed_state.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_size_t]
+    L.qmhd_solver_state_component_to_host.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_size_t]
+    L.qmhd_solver_cfl_limit.argtypes = [vp, dp]
+    L.qmhd_solver_step.argtypes = [vp, ctypes.c_double]
+    L.qmhd_solver_step_unchecked.argtypes = [vp, ctypes.c_double]
+    L.qmhd_solver_advance.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    L.qmhd_solver_divergence_b_max.argtypes = [vp, dp]
+    L.qmhd_solver_conserved_cell_totals.argtypes = [vp, dp, dp]
+    L.qmhd_solver_last_positivity_substeps.argtypes = [vp]
+    L.qmhd_solver_advance_auto.argtypes = [vp, dp, ctypes.c_double, ctypes.c_int, ip]
+    L.qmhd_solver_time_auto_steps.argtypes = [vp, ctypes.c_int, dp, ip]
+    L.qmhd_solver_profile_step.argtypes = [vp, dp, ctypes.c_int]
+    L.qmhd_fp64_fma_peak.argtypes = [dp]
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    """Map a C status to the exception the reference's binding raises."""
+    if rc == QMHD_OK:
+        return
+    msg = lib().qmhd_last_error().decode()
+    if rc == QMHD_INVALID_ARGUMENT:
+        raise ValueError(msg)
+    raise RuntimeError(msg)

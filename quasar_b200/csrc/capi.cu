@@ -1,0 +1,212 @@
+// extern "C" boundary over qb::MhdSolver2D (declarations: include/quasar_mhd.h).
+#include "../../include/quasar_mhd.h"
+#include "../../include/quasar_mhd_ext.h"
+#include "mhd_solver.cuh"
+
+#include <cstring>
+#include <exception>
+#include <stdexcept>
+#include <string>
+
+namespace qb {
+double fp64_fma_peak_tflops();
+}
+
+struct qmhd_solver {
+  qb::MhdSolver2D impl;
+  explicit qmhd_solver(const qb::Config& c) : impl(c) {}
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_error.clear();
+    return QMHD_OK;
+  } catch (const qb::CudaError& e) {
+    g_error = e.what();
+    return QMHD_DEVICE_ERROR;
+  } catch (const std::invalid_argument& e) {
+    g_error = e.what();
+    return QMHD_INVALID_ARGUMENT;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return QMHD_RUNTIME_ERROR;
+  } catch (...) {
+    g_error = "unknown error";
+    return QMHD_RUNTIME_ERROR;
+  }
+}
+
+// Component spellings of MhdSolver2D::component_buffer (mhd_solver.cpp:507-519).
+// Reads of "bx"/"by" return the collocated field (indices 8/9).
+int component_index(const char* name, bool for_read) {
+  if (!name) throw std::invalid_argument("MhdSolver2D: unknown state component ''");
+  const std::string c(name);
+  if (c == "rho") return 0;
+  if (c == "mx") return 1;
+  if (c == "my") return 2;
+  if (c == "mz") return 3;
+  if (c == "energy") return 4;
+  if (c == "bx") return for_read ? 8 : 5;
+  if (c == "bx_face") return 5;
+  if (c == "by") return for_read ? 9 : 6;
+  if (c == "by_face") return 6;
+  if (c == "bz" || c == "bz_cell") return 7;
+  throw std::invalid_argument("MhdSolver2D: unknown state component '" + c + "'");
+}
+
+void need(const void* p) {
+  if (!p) throw std::invalid_argument("qmhd: null pointer argument");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* qmhd_last_error(void) { return g_error.c_str(); }
+
+int qmhd_solver_create(const qmhd_config* config, qmhd_solver** out) {
+  return guarded([&] {
+    need(config);
+    need(out);
+    *out = nullptr;
+    qb::Config c;
+    c.nx = config->nx;
+    c.ny = config->ny;
+    c.lx = config->lx;
+    c.ly = config->ly;
+    c.ox = config->origin_x;
+    c.oy = config->origin_y;
+    c.order = config->reconstruction_order;
+    c.gamma = config->gamma;
+    c.cfl = config->cfl;
+    for (int s = 0; s < 4; ++s) c.bc[s] = config->boundary[s];
+    *out = new qmhd_solver(c);
+  });
+}
+
+void qmhd_solver_destroy(qmhd_solver* solver) { delete solver; }
+
+int qmhd_solver_grid(const qmhd_solver* s, int* nx, int* ny, int* nghost) {
+  return guarded([&] {
+    need(s);
+    const qb::Grid& g = s->impl.grid();
+    if (nx) *nx = g.nx;
+    if (ny) *ny = g.ny;
+    if (nghost) *nghost = g.ng;
+  });
+}
+
+long long qmhd_solver_storage_size(const qmhd_solver* s) {
+  return s ? s->impl.storage_size() : -1;
+}
+
+int qmhd_solver_seed_state(qmhd_solver* s, const char* component, const double* values,
+                           size_t n) {
+  return guarded([&] {
+    need(s);
+    need(values);
+    s->impl.seed_state(component_index(component, false), values, (long long)n);
+  });
+}
+
+int qmhd_solver_state_component_to_host(qmhd_solver* s, const char* component, double* out,
+                                        size_t n) {
+  return guarded([&] {
+    need(s);
+    need(out);
+    s->impl.state_component_to_host(component_index(component, true), out, (long long)n);
+  });
+}
+
+int qmhd_solver_cfl_limit(qmhd_solver* s, double* dt) {
+  return guarded([&] {
+    need(s);
+    need(dt);
+    *dt = s->impl.cfl_limit();
+  });
+}
+
+int qmhd_solver_step(qmhd_solver* s, double dt) {
+  return guarded([&] {
+    need(s);
+    s->impl.step(dt);
+  });
+}
+
+int qmhd_solver_step_unchecked(qmhd_solver* s, double dt) {
+  return guarded([&] {
+    need(s);
+    s->impl.step_unchecked(dt);
+  });
+}
+
+int qmhd_solver_advance(qmhd_solver* s, double t_end, double dt) {
+  return guarded([&] {
+    need(s);
+    s->impl.advance(t_end, dt);
+  });
+}
+
+int qmhd_solver_divergence_b_max(qmhd_solver* s, double* out) {
+  return guarded([&] {
+    need(s);
+    need(out);
+    *out = s->impl.divergence_b_max();
+  });
+}
+
+int qmhd_solver_conserved_cell_totals(qmhd_solver* s, double* mass, double* energy) {
+  return guarded([&] {
+    need(s);
+    need(mass);
+    need(energy);
+    s->impl.conserved_cell_totals(mass, energy);
+  });
+}
+
+int qmhd_solver_last_positivity_substeps(const qmhd_solver* s) {
+  return s ? s->impl.last_positivity_substeps() : -1;
+}
+
+int qmhd_solver_advance_auto(qmhd_solver* s, double* t, double t_end, int max_steps,
+                             int* steps_taken) {
+  return guarded([&] {
+    need(s);
+    need(t);
+    const int n = s->impl.advance_auto(t, t_end, max_steps);
+    if (steps_taken) *steps_taken = n;
+  });
+}
+
+int qmhd_solver_time_auto_steps(qmhd_solver* s, int steps, double* ms, int* done) {
+  return guarded([&] {
+    need(s);
+    need(ms);
+    *ms = s->impl.time_auto_steps(steps, done);
+  });
+}
+
+int qmhd_solver_profile_step(qmhd_solver* s, double* ms, int n) {
+  return guarded([&] {
+    need(s);
+    need(ms);
+    if (n < qb::MhdSolver2D::kPhases) throw std::invalid_argument("qmhd: phase buffer too small");
+    s->impl.profile_step(ms);
+  });
+}
+
+int qmhd_fp64_fma_peak(double* tflops) {
+  return guarded([&] {
+    need(tflops);
+    *tflops = qb::fp64_fma_peak_tflops();
+    if (!(*tflops > 0.0)) throw qb::CudaError("FP64 probe failed");
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+// Host side of the B200 MHD solver: the reference's MhdSolver2D interface
+// (physics/mhd/mhd_solver.hpp:85-173) over the sm_100a kernels.
+//
+// Device memory is allocated once, at construction; stepping allocates
+// nothing.  Four state registers rotate (live U^n, stage outputs U1, U2 and
+// the next state), so the Shu-Osher combine never needs a rollback copy: a
+// rejected candidate is simply not promoted.  dt, the CFL reduction and the
+// admissibility fractions live in a device control block; the API-mode step
+// reads back one status word, the device-resident loop none.
+#pragma once
+
+#include "mhd_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+
+namespace qb {
+
+struct Config {
+  int nx = 0, ny = 0;
+  double lx = 1.0, ly = 1.0, ox = 0.0, oy = 0.0;
+  int order = 7;  // 2 (muscl_minmod), 5 (mp5), 7 (mp7)
+  double gamma = 5.0 / 3.0;
+  double cfl = 0.4;
+  int bc[4] = {0, 0, 0, 0};  // x_lo, x_hi, y_lo, y_hi: 0 periodic, 1 outflow, 2 wall
+};
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+class MhdSolver2D {
+ public:
+  explicit MhdSolver2D(const Config& cfg);
+  ~MhdSolver2D();
+  MhdSolver2D(const MhdSolver2D&) = delete;
+  MhdSolver2D& operator=(const MhdSolver2D&) = delete;
+
+  const Grid& grid() const { return g_; }
+  const Config& config() const { return cfg_; }
+  long long storage_size() const { return g_.size(); }
+
+  // Reference-facing API (mhd_solver.hpp:111-173).
+  void seed_state(int comp, const double* host, long long n);
+  // comp 0..7 raw storage; 8 / 9 = the collocated cell bx / by.
+  void state_component_to_host(int comp, double* host, long long n);
+  double cfl_limit();
+  void step(double dt);
+  void step_unchecked(double dt);
+  void advance(double t_end, double dt);
+  double divergence_b_max();
+  void conserved_cell_totals(double* mass, double* energy);
+  int last_positivity_substeps() const { return last_substeps_; }
+
+  // Device-resident auto-dt loop: up to `max_steps` steps of
+  // dt = min(cfl_limit, t_end - t) without host round trips (replayed CUDA
+  // graphs); a step the positivity controller must retry falls back to the
+  // host controller.  Returns the steps taken; *t is advanced in place.
+  int advance_auto(double* t, double t_end, int max_steps);
+
+  // Measurement hooks (bench.py): `steps` device-resident auto-dt steps timed
+  // with CUDA events on the solver stream (returns ms, *done = steps taken),
+  // and one API step with per-phase device times (ms_by_phase[kPhases]).
+  double time_auto_steps(int steps, int* done);
+  void profile_step(double* ms_by_phase);
+  static constexpr int kPhases = 8;
+
+  // Device pointers of the live state (kernel-level C-ABI and tests).
+  double* live_component(int comp) const;
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  struct Attempt {
+    bool ok;
+    double theta;
+  };
+  StageArgs stage_args(const StateP& u, int order) const;
+  void ensure_live_ready();
+  void refresh_live_stats();
+  void front_impl(int order, int dt_mode, int anchor_mode);
+  void finish_impl(int order, const double* dt_dev, double dt_host, bool step_end);
+  Ctl read_ctl();
+  void throw_status(int status);
+  void promote();
+  void copy_state(const StateP& src, const StateP& dst);
+  void advance_positive(double dt);
+  void controller(double dt, double theta, bool anchor);
+  double cfl_limit_for(int coll);
+  void check_cuda(const char* what);
+  void build_graphs();
+
+  Config cfg_;
+  Grid g_;
+  cudaStream_t stream_ = nullptr;
+  double* arena_ = nullptr;
+  int* iarena_ = nullptr;
+  Ctl* ctl_ = nullptr;
+  Ctl* ctl_host_ = nullptr;  // pinned mirror
+  double* sums_ = nullptr;
+  unsigned long long* scalar_ = nullptr;
+  int sum_blocks_ = 0;
+  StateP st_[5];  // 0..3 rotating registers, 4 = request backup
+  int live_ = 0, s1_ = 1, s2_ = 2, next_ = 3;
+  IfaceP ix_, iy_;
+  FluxP fx_, fy_;
+  double *xemf_, *yemf_, *xspd_, *yspd_, *cell_ez_, *ez_;
+  int *xnj_, *ynj_;
+  bool seeded_dirty_ = true;    // live state written externally since last check
+  bool solver_owned_ = false;   // live state produced by an accepted step
+  int front_order_ = 0;         // order of the cached stage-0 residual (0 = none)
+  int front_dt_mode_ = 0;       // whether that residual also produced a device dt
+  int anchor_mode_ = -1;        // forced low-order anchor flag inside the controller
+  int low_order_ = 0;           // 1 while the positivity controller runs low order
+  int last_substeps_ = 0;
+  cudaGraphExec_t graph_[2] = {nullptr, nullptr};
+  // per-phase event marks while profiling (phase, event after the launch)
+  struct Mark {
+    int phase;
+    cudaEvent_t ev;
+  };
+  Mark* marks_ = nullptr;
+  int nmarks_ = 0;
+  void mark(int phase);
+};
+
+}  // namespace qb

@@ -1,0 +1,186 @@
+"""Python mirror of the reference's `_core.mhd` module
+(bindings/python/bind_mhd.cpp:571-647) over the sm_100a C ABI.
+
+    cfg = MhdConfig()
+    cfg.grid = Grid2D(256, 256, 1.0, 1.0)
+    cfg.reconstruction = "mp7"
+    solver = MhdSolver2D(cfg)
+    solver.seed_state("rho", rho_padded)      # storage-sized float64 arrays
+    dt = solver.cfl_limit(); solver.step_unchecked(dt)
+    rho = solver.state_component_to_host("rho")
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import List
+
+import numpy as np
+
+from . import _native
+
+_ORDERS = {"muscl_minmod": 2, "mp5": 5, "mp7": 7}
+_BC = {"periodic": 0, "outflow": 1, "wall": 2}
+
+
+@dataclass
+class Grid2D:
+    """core/grid.hpp:84-161 (nghost 0 lets the solver size the halo)."""
+    nx: int = 1
+    ny: int = 1
+    lx: float = 1.0
+    ly: float = 1.0
+    origin_x: float = 0.0
+    origin_y: float = 0.0
+    nghost: int = 0
+
+    def dx(self) -> float:
+        return self.lx / self.nx
+
+    def dy(self) -> float:
+        return self.ly / self.ny
+
+    def pitch(self) -> int:
+        return self.nx + 2 * self.nghost
+
+    def storage_size(self) -> int:
+        return (self.nx + 2 * self.nghost) * (self.ny + 2 * self.nghost)
+
+
+@dataclass
+class MhdBoundarySpec:
+    """boundary/mhd_boundary.hpp: per-side registry names, [x_lo,x_hi,y_lo,y_hi]."""
+    fluid: List[str] = field(default_factory=lambda: ["periodic"] * 4)
+    field: List[str] = field(default_factory=lambda: ["periodic"] * 4)
+
+
+@dataclass
+class MhdConfig:
+    """physics/mhd/mhd_solver.hpp:50-83."""
+    grid: Grid2D = field(default_factory=Grid2D)
+    gamma: float = 5.0 / 3.0
+    geometry: str = "cartesian"
+    reconstruction: str = "mp7"
+    riemann: str = "hlld"
+    integrator: str = "ssprk3"
+    ct: str = "fd_ct_christlieb"
+    positivity: str = "troubled_cell"
+    rho_floor: float = 1e-8
+    p_floor: float = 1e-9
+    cfl: float = 0.4
+    boundary: MhdBoundarySpec = field(default_factory=MhdBoundarySpec)
+
+
+def _native_config(cfg: MhdConfig) -> _native.QmhdConfig:
+    if cfg.geometry != "cartesian":
+        raise ValueError("MhdSolver2D: geometry must be 'cartesian' in this build")
+    if cfg.riemann != "hlld":
+        raise ValueError("MhdSolver2D: device evolution supports only riemann='hlld'")
+    if cfg.ct != "fd_ct_christlieb":
+        raise ValueError("MhdSolver2D: device evolution supports only ct='fd_ct_christlieb'")
+    if cfg.integrator != "ssprk3":
+        raise ValueError(f"MhdSolver2D: unknown integrator '{cfg.integrator}'")
+    if cfg.positivity != "troubled_cell":
+        raise ValueError(f"MhdSolver2D: unknown positivity limiter '{cfg.positivity}'")
+    if cfg.reconstruction not in _ORDERS:
+        raise ValueError(
+            "MhdSolver2D: device evolution supports only reconstruction='muscl_minmod', "
+            "'mp5', or 'mp7'")
+    order = _ORDERS[cfg.reconstruction]
+    required = 4 if order == 7 else 3 if order == 5 else 2
+    if cfg.grid.nghost > 0 and cfg.grid.nghost != required:
+        raise ValueError(
+            f"MhdSolver2D: grid nghost ({cfg.grid.nghost}) must equal the reconstruction "
+            f"scheme's halo ({required}) in this build")
+    bc = []
+    for side in range(4):
+        f, b = cfg.boundary.fluid[side], cfg.boundary.field[side]
+        if f not in _BC or b not in _BC:
+            raise ValueError(f"MhdSolver2D: unknown boundary '{f if f not in _BC else b}'")
+        if f != b:
+            raise ValueError("MhdSolver2D: fluid and field boundaries must match per side in this build")
+        bc.append(_BC[f])
+    c = _native.QmhdConfig()
+    c.nx, c.ny = int(cfg.grid.nx), int(cfg.grid.ny)
+    c.lx, c.ly = float(cfg.grid.lx), float(cfg.grid.ly)
+    c.origin_x, c.origin_y = float(cfg.grid.origin_x), float(cfg.grid.origin_y)
+    c.reconstruction_order = order
+    c.gamma = float(cfg.gamma)
+    c.cfl = float(cfg.cfl)
+    for s in range(4):
+        c.boundary[s] = bc[s]
+    return c
+
+
+class MhdSolver2D:
+    """physics/mhd/mhd_solver.hpp:85-173 on the sm_100a kernels."""
+
+    def __init__(self, config: MhdConfig):
+        L = _native.lib()
+        self._cfg = config
+        h = ctypes.c_void_p()
+        _native.check(L.qmhd_solver_create(ctypes.byref(_native_config(config)), ctypes.byref(h)))
+        self._h = h
+        nx, ny, ng = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _native.check(L.qmhd_solver_grid(self._h, ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(ng)))
+        g = config.grid
+        self._grid = Grid2D(nx.value, ny.value, g.lx, g.ly, g.origin_x, g.origin_y, ng.value)
+        self._n = int(L.qmhd_solver_storage_size(self._h))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _native.lib().qmhd_solver_destroy(h)
+            self._h = None
+
+    def grid(self) -> Grid2D:
+        return self._grid
+
+    def config(self) -> MhdConfig:
+        return self._cfg
+
+    def seed_state(self, component: str, values) -> None:
+        a = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1))
+        _native.check(_native.lib().qmhd_solver_seed_state(
+            self._h, component.encode(), a.ctypes.data, a.size))
+
+    def state_component_to_host(self, component: str) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.float64)
+        _native.check(_native.lib().qmhd_solver_state_component_to_host(
+            self._h, component.encode(), out.ctypes.data, out.size))
+        return out
+
+    def cfl_limit(self) -> float:
+        d = ctypes.c_double()
+        _native.check(_native.lib().qmhd_solver_cfl_limit(self._h, ctypes.byref(d)))
+        return d.value
+
+    def step(self, dt: float) -> None:
+        _native.check(_native.lib().qmhd_solver_step(self._h, float(dt)))
+
+    def step_unchecked(self, dt: float) -> None:
+        _native.check(_native.lib().qmhd_solver_step_unchecked(self._h, float(dt)))
+
+    def advance(self, t_end: float, dt: float) -> None:
+        _native.check(_native.lib().qmhd_solver_advance(self._h, float(t_end), float(dt)))
+
+    def divergence_b_max(self) -> float:
+        d = ctypes.c_double()
+        _native.check(_native.lib().qmhd_solver_divergence_b_max(self._h, ctypes.byref(d)))
+        return d.value
+
+    def conserved_cell_totals(self):
+        m, e = ctypes.c_double(), ctypes.c_double()
+        _native.check(_native.lib().qmhd_solver_conserved_cell_totals(
+            self._h, ctypes.byref(m), ctypes.byref(e)))
+        return (m.value, e.value)
+
+    def last_positivity_substeps(self) -> int:
+        return int(_native.lib().qmhd_solver_last_positivity_substeps(self._h))
+
+    def advance_auto(self, t: float, t_end: float, max_steps: int):
+        """Device-resident auto-dt loop; returns (t, steps_taken)."""
+        tt, n = ctypes.c_double(float(t)), ctypes.c_int()
+        _native.check(_native.lib().qmhd_solver_advance_auto(
+            self._h, ctypes.byref(tt), float(t_end), int(max_steps), ctypes.byref(n)))
+        return tt.value, n.value

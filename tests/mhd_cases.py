@@ -10,8 +10,8 @@ bz_cell.
 from __future__ import annotations
 
 import ctypes
-import math
 import os
+import sys
 
 import numpy as np
 
@@ -28,78 +28,10 @@ def nghost(order: int) -> int:
     return 4 if order == 7 else 3 if order == 5 else 2
 
 
-# --------------------------------------------------------------------------
-# Initial states (primitive profiles -> conserved, face-sampled B).
-# --------------------------------------------------------------------------
-def _centres(n, ng, length, origin=0.0):
-    i = np.arange(-ng, n + ng, dtype=np.float64)
-    d = length / n
-    return (i + 0.5) * d + origin
-
-
-def _assemble(rho, vx, vy, vz, p, bx, by, bz, gamma):
-    kin = 0.5 * rho * (vx * vx + vy * vy + vz * vz)
-    mag = 0.5 * (bx * bx + by * by + bz * bz)
-    energy = p / (gamma - 1.0) + kin + mag
-    return [np.ascontiguousarray(a, dtype=np.float64) for a in
-            (rho, rho * vx, rho * vy, rho * vz, energy, bx, by, bz)]
-
-
-def orszag_tang(n, order=5, gamma=5.0 / 3.0, amplitude=1.0, ny=None):
-    """Orszag-Tang on [0,1]^2: rho=25/(36 pi), p=5/(12 pi),
-    v=(-sin 2 pi y, sin 2 pi x), face B = B0 (-sin 2 pi y, sin 4 pi x),
-    B0 = 1/sqrt(4 pi).  `amplitude` scales rho, p by a and B by sqrt(a)."""
-    ny = n if ny is None else ny
-    ng = nghost(order)
-    x = _centres(n, ng, 1.0)
-    y = _centres(ny, ng, 1.0)
-    X, Y = np.meshgrid(x, y, indexing="xy")
-    pi = math.pi
-    a = amplitude
-    rho = np.full_like(X, a * 25.0 / (36.0 * pi))
-    p = np.full_like(X, a * 5.0 / (12.0 * pi))
-    b0 = math.sqrt(a) / math.sqrt(4.0 * pi)
-    vx = -np.sin(2 * pi * Y)
-    vy = np.sin(2 * pi * X)
-    bx = -b0 * np.sin(2 * pi * Y)
-    by = b0 * np.sin(4 * pi * X)
-    z = np.zeros_like(X)
-    return _assemble(rho, vx, vy, z, p, bx, by, z, gamma)
-
-
-def rotor(n, order=7, gamma=5.0 / 3.0):
-    """MHD rotor on [0,1]^2: rho=10 inside r<0.1, linear taper to 1 at
-    r=0.115, angular velocity 20 inside (u0=2, r0=0.1), p=1, Bx=5/sqrt(4 pi)."""
-    ng = nghost(order)
-    x = _centres(n, ng, 1.0)
-    X, Y = np.meshgrid(x, x, indexing="xy")
-    rx, ry = X - 0.5, Y - 0.5
-    r = np.hypot(rx, ry)
-    r0, r1, u0 = 0.1, 0.115, 2.0
-    f = np.clip((r1 - r) / (r1 - r0), 0.0, 1.0)
-    f = np.where(r <= r0, 1.0, np.where(r >= r1, 0.0, f))
-    with np.errstate(divide="ignore", invalid="ignore"):
-        sf = np.where(r <= r0, u0 / r0, np.where(r < r1, f * u0 / np.maximum(r, 1e-300), 0.0))
-    rho = 1.0 + f * (10.0 - 1.0)
-    vx, vy = -sf * ry, sf * rx
-    p = np.ones_like(X)
-    z = np.zeros_like(X)
-    bx = np.full_like(X, 5.0 / math.sqrt(4.0 * math.pi))
-    return _assemble(rho, vx, vy, z, p, bx, z, z, gamma)
-
-
-def blast(n, order=7, gamma=5.0 / 3.0):
-    """MHD blast on [0,1]^2: p=100 for r<0.1 else 0.1, rho=1,
-    Bx=By=10/sqrt(8 pi)."""
-    ng = nghost(order)
-    x = _centres(n, ng, 1.0)
-    X, Y = np.meshgrid(x, x, indexing="xy")
-    r = np.hypot(X - 0.5, Y - 0.5)
-    p = np.where(r < 0.1, 100.0, 0.1)
-    rho = np.ones_like(X)
-    b = 10.0 / math.sqrt(8.0 * math.pi)
-    z = np.zeros_like(X)
-    return _assemble(rho, z, z, z, p, np.full_like(X, b), np.full_like(X, b), z, gamma)
+# Initial states: the product's generators (quasar_b200/ics.py), so the
+# checkers and the CUDA path are always seeded with the same arrays.
+sys.path.insert(0, ROOT)
+from quasar_b200.ics import blast, orszag_tang, rotor  # noqa: E402,F401
 
 
 # --------------------------------------------------------------------------
@@ -221,6 +153,7 @@ class OracleLib(_Lib):
                                  ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.qor_residual.argtypes = [ctypes.c_void_p] * 9
         L.qor_count_flops.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
+        L.qor_count_phases.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
 
     def solver(self, nx, ny, order, gamma=5.0 / 3.0, cfl=0.4, bc=PERIODIC, lx=1.0, ly=1.0, counting=False):
         h = self.lib.qor_create(nx, ny, lx, ly, order, gamma, cfl, (ctypes.c_int * 4)(*bc), int(counting))
@@ -229,9 +162,16 @@ class OracleLib(_Lib):
         return CpuSolver(self, h, nx, ny, order)
 
     def count_flops(self, solver: CpuSolver, steps: int):
+        """(as written, algorithmic, CFL share) FLOPs per zone-step."""
         a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         solver._call("count_flops", steps, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
         return a.value, b.value, c.value
+
+    def count_phases(self, solver: CpuSolver, steps: int):
+        """Algorithmic FLOPs per zone-step by phase (see qor_count_phases)."""
+        out = np.zeros(8)
+        solver._call("count_phases", steps, out.ctypes.data)
+        return out
 
 
 class RefLib(_Lib):

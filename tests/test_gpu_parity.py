@@ -1,0 +1,163 @@
+"""Parity of the sm_100a product against the oracle restatement and the
+reference's own solver (committed fixtures), through the C ABI.
+
+Bars (stated by the task for this path): per-step state within 1e-10
+relative L1 (per physical group: rho, momentum, energy, field), dt equal to
+the reference's to 1e-12 relative, div B at round-off (<= 1e-12)."""
+import os
+
+import numpy as np
+import pytest
+
+import mhd_cases as M
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = {"ot": M.orszag_tang, "rotor": M.rotor, "blast": M.blast}
+ORDER_NAME = {2: "muscl_minmod", 5: "mp5", 7: "mp7"}
+BC_NAME = {0: "periodic", 1: "outflow", 2: "wall"}
+STEP_TOL = 1e-10
+DT_TOL = 1e-12
+
+
+def gpu_solver(n, order, bc=M.PERIODIC, gamma=5.0 / 3.0, cfl=0.4, ny=None):
+    from quasar_b200 import mhd
+    cfg = mhd.MhdConfig()
+    cfg.grid = mhd.Grid2D(n, ny or n, 1.0, 1.0)
+    cfg.reconstruction = ORDER_NAME[order]
+    cfg.gamma = gamma
+    cfg.cfl = cfl
+    cfg.boundary = mhd.MhdBoundarySpec([BC_NAME[b] for b in bc], [BC_NAME[b] for b in bc])
+    return mhd.MhdSolver2D(cfg)
+
+
+def seed(s, comps):
+    for name, a in zip(M.COMPONENTS, comps):
+        s.seed_state(name, a)
+
+
+def read(s, shape):
+    return [s.state_component_to_host(c).reshape(shape) for c in M.COMPONENTS]
+
+
+def load_fixture(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize("name", ["ot32_mp5", "ot32_mp7", "rotor32_mp7", "blast32_mp7",
+                                  "rotor48_mp5", "ot24_muscl"])
+def test_steps_match_oracle_and_reference(oracle, name):
+    fx = load_fixture(name)
+    n, order, case = int(fx["n"]), int(fx["order"]), str(fx["case"])
+    bc = tuple(int(b) for b in fx["bc"])
+    ic = CASES[case](n, order=order)
+    g = gpu_solver(n, order, bc)
+    o = oracle.solver(n, n, order, bc=bc)
+    seed(g, ic)
+    o.seed(ic)
+    ng = M.nghost(order)
+    shape = (n + 2 * ng, n + 2 * ng)
+    for k, dt_ref in enumerate(fx["dts"]):
+        dt = g.cfl_limit()
+        assert abs(dt - dt_ref) <= DT_TOL * dt_ref, (k, dt, dt_ref)
+        g.step_unchecked(dt_ref)
+        o.step(dt_ref)
+        err = M.state_rel_l1(read(g, shape), o.read(), ng, n, n)
+        assert err <= STEP_TOL, (k, err)
+    final = read(g, shape)
+    want = [fx[c] for c in M.COMPONENTS]
+    assert M.state_rel_l1(final, want, ng, n, n) <= STEP_TOL * len(fx["dts"])
+    assert g.divergence_b_max() <= 1e-12
+
+
+def test_divb_roundoff_and_conservation():
+    n, order = 64, 5
+    g = gpu_solver(n, order)
+    seed(g, M.orszag_tang(n, order=order))
+    m0, e0 = g.conserved_cell_totals()
+    for _ in range(20):
+        g.step_unchecked(g.cfl_limit())
+    m1, e1 = g.conserved_cell_totals()
+    assert abs(m1 - m0) <= 1e-12 * abs(m0)
+    assert abs(e1 - e0) <= 1e-12 * abs(e0)
+    assert g.divergence_b_max() <= 1e-12
+
+
+def test_device_resident_loop_equals_api_loop():
+    n, order = 48, 7
+    ic = M.rotor(n, order=order)
+    a, b = gpu_solver(n, order, M.OUTFLOW), gpu_solver(n, order, M.OUTFLOW)
+    seed(a, ic)
+    seed(b, ic)
+    t_end = 1e9
+    t, steps = a.advance_auto(0.0, t_end, 7)
+    assert steps == 7
+    tb = 0.0
+    for _ in range(7):
+        dt = b.cfl_limit()
+        b.step_unchecked(dt)
+        tb += dt
+    assert t == tb
+    shape = (n + 8, n + 8)
+    for x, y in zip(read(a, shape), read(b, shape)):
+        assert np.array_equal(x, y)
+
+
+def test_device_resident_loop_stops_at_t_end():
+    n, order = 32, 5
+    g = gpu_solver(n, order)
+    seed(g, M.orszag_tang(n, order=order))
+    t, steps = g.advance_auto(0.0, 0.01, 1000)
+    assert t == 0.01 and 0 < steps < 1000
+
+
+def test_positivity_retry_matches_oracle(oracle):
+    n, order = 16, 5
+    ic = M.blast(n, order=order)
+    ic[4] = np.where(ic[4] > 100, ic[4] * 1e3, ic[4])
+    g, o = gpu_solver(n, order, M.OUTFLOW), oracle.solver(n, n, order, bc=M.OUTFLOW)
+    seed(g, ic)
+    o.seed(ic)
+    dt = 3.0 * o.cfl()
+    g.step_unchecked(dt)
+    o.step(dt)
+    assert g.last_positivity_substeps() == o.substeps() >= 2
+    shape = (n + 6, n + 6)
+    assert M.state_rel_l1(read(g, shape), o.read(), 3, n, n) <= STEP_TOL
+
+
+def test_error_behaviour_matches_reference():
+    n, order = 16, 5
+    g = gpu_solver(n, order)
+    ic = M.orszag_tang(n, order=order)
+    bad = [a.copy() for a in ic]
+    bad[0][5, 5] = np.nan
+    with pytest.raises(ValueError):
+        g.seed_state("rho", bad[0])
+    with pytest.raises(ValueError):
+        g.seed_state("rho", ic[0][:-1])
+    with pytest.raises(ValueError):
+        g.seed_state("temperature", ic[0])
+    # inadmissible live state: negative pressure in one interior cell
+    seed(g, ic)
+    e = ic[4].copy()
+    e[8, 8] = -1.0
+    g.seed_state("energy", e)
+    with pytest.raises(ValueError):
+        g.cfl_limit()
+    # non-solenoidal face field
+    seed(g, ic)
+    bx = ic[5].copy()
+    bx[8, 8] += 0.1
+    g.seed_state("bx_face", bx)
+    with pytest.raises(ValueError):
+        g.step_unchecked(1e-4)
+    # recover: a valid seed steps again
+    seed(g, ic)
+    g.step_unchecked(g.cfl_limit())
+    with pytest.raises(ValueError):
+        g.step_unchecked(-1.0)
+    with pytest.raises(ValueError):
+        g.step(10.0 * g.cfl_limit())
