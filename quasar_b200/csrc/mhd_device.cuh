@@ -140,6 +140,26 @@ __device__ __forceinline__ double pressure(const St& u, double gamma) {
   const double m = half_sq3(u.bx, u.by, u.bz);
   return mul(sub(gamma, 1.0), sub(sub(u.E, k), m));
 }
+// Plain-arithmetic EOS for the places whose result depends continuously on
+// rounding (Riemann solver, CFL speeds, admissibility tests): one reciprocal
+// of rho instead of the reference's component-scaled forms, which only guard
+// binary64 overflow for |state| near 1e154 (outside every configuration here).
+__device__ __forceinline__ double pressure_f(const St& u, double gamma, double ir) {
+  const double k = 0.5 * ((u.mx * u.mx + u.my * u.my + u.mz * u.mz) * ir);
+  const double m = 0.5 * (u.bx * u.bx + u.by * u.by + u.bz * u.bz);
+  return (gamma - 1.0) * ((u.E - k) - m);
+}
+// fast magnetosonic speed normal to x from p and 1/rho (mhd_state.hpp:148-182)
+__device__ __forceinline__ double fast_x_f(const St& u, double p, double ir, double gamma) {
+  const double a2 = p > 0.0 ? gamma * p * ir : 0.0;
+  const double bn2 = u.bx * u.bx * ir;
+  const double b2 = (u.bx * u.bx + u.by * u.by + u.bz * u.bz) * ir;
+  const double sum = a2 + b2;
+  double disc = sum * sum - 4.0 * a2 * bn2;
+  if (disc < 0.0) disc = 0.0;
+  return sqrt(0.5 * (sum + sqrt(disc)));
+}
+
 __device__ __forceinline__ Pr to_prim(const St& u, double gamma) {
   Pr w;
   w.rho = u.rho;
@@ -185,8 +205,10 @@ __device__ __forceinline__ St swap_xy(const St& v) {
 // Finite, rho>0, finite velocity, p>0 (mhd_reconstruct.hip:414-427).
 __device__ __forceinline__ bool recon_admissible(const St& s, double gamma) {
   if (!(isfinite(s.rho) && s.rho > 0.0)) return false;
-  const Pr w = to_prim(s, gamma);
-  if (!(isfinite(w.vx) && isfinite(w.vy) && isfinite(w.vz) && isfinite(w.p) && w.p > 0.0))
+  const double ir = 1.0 / s.rho;
+  const double p = pressure_f(s, gamma, ir);
+  if (!(isfinite(s.mx * ir) && isfinite(s.my * ir) && isfinite(s.mz * ir) && isfinite(p) &&
+        p > 0.0))
     return false;
   return isfinite(s.mx) && isfinite(s.my) && isfinite(s.mz) && isfinite(s.E) &&
          isfinite(s.bx) && isfinite(s.by) && isfinite(s.bz);
@@ -197,7 +219,7 @@ __device__ __forceinline__ bool point_admissible(const St& s, double gamma) {
         isfinite(s.mz) && isfinite(s.E) && isfinite(s.bx) && isfinite(s.by) &&
         isfinite(s.bz)))
     return false;
-  const double p = pressure(s, gamma);
+  const double p = pressure_f(s, gamma, 1.0 / s.rho);
   return isfinite(p) && p > 0.0;
 }
 
@@ -213,7 +235,9 @@ __device__ __forceinline__ double minmod4(double a, double b, double c, double d
   const double m = fmin(fmin(fabs(a), fabs(b)), fmin(fabs(c), fabs(d)));
   return sa > 0 ? m : -m;
 }
-// mp_limiter.hpp:71-148.  `*fired` is set when the candidate was changed.
+// mp_limiter.hpp:71-148.  `fired` is set when the candidate was changed.
+// The normalisations by the local variation and the curvature scale use one
+// reciprocal each instead of a division per term (rounding-level difference).
 __device__ __forceinline__ double mp_limit(double vl, double vm2, double vm1, double v0,
                                            double vp1, double vp2, bool& fired) {
   const double dmn = v0 - vm1;
@@ -222,7 +246,11 @@ __device__ __forceinline__ double mp_limit(double vl, double vm2, double vm1, do
   const double cc = vl - v0, cm = vl - vmp;
   const bool between = (cc <= 0.0 && cm >= 0.0) || (cc >= 0.0 && cm <= 0.0);
   const double var = fmax(fmax(fabs(dmn), fabs(dpl)), fmax(fabs(cc), fabs(cm)));
-  const bool roundoff = var > 0.0 && (fabs(cc) / var) * (fabs(cm) / var) <= 1e-10;
+  bool roundoff = false;
+  if (!between && var > 0.0) {
+    const double iv = 1.0 / var;
+    roundoff = (fabs(cc) * iv) * (fabs(cm) * iv) <= 1e-10;
+  }
   if (between || roundoff) {
     fired = false;
     return vl;
@@ -234,7 +262,8 @@ __device__ __forceinline__ double mp_limit(double vl, double vm2, double vm1, do
   const double cs = fmax(fabs(dm), fmax(fabs(d0), fabs(dp)));
   double d4ph = 0.0, d4mh = 0.0;
   if (cs > 0.0) {
-    const double dms = dm / cs, d0s = d0 / cs, dps = dp / cs;
+    const double ic = 1.0 / cs;
+    const double dms = dm * ic, d0s = d0 * ic, dps = dp * ic;
     d4ph = cs * minmod4(4.0 * d0s - dps, 4.0 * dps - d0s, d0s, dps);
     d4mh = cs * minmod4(4.0 * d0s - dms, 4.0 * dms - d0s, d0s, dms);
   }
@@ -246,7 +275,8 @@ __device__ __forceinline__ double mp_limit(double vl, double vm2, double vm1, do
   const double vmax = fmin(fmax(fmax(v0, vp1), v_md), fmax(fmax(v0, v_ul), v_lc));
   return vl + minmod2(vmin - vl, vmax - vl);
 }
-// mp_limiter.hpp:182-224: W = 5 (MP5) or 7 (MP7); v[0..W-1].
+// mp_limiter.hpp:182-224: W = 5 (MP5) or 7 (MP7); v[0..W-1].  The stencil is
+// normalised by its largest magnitude through one reciprocal.
 template <int W>
 __device__ __forceinline__ double mp_recon(const double* v, bool& fired) {
   double s = 0.0;
@@ -255,27 +285,29 @@ __device__ __forceinline__ double mp_recon(const double* v, bool& fired) {
   double vl;
   if (s == 0.0) {
     vl = 0.0;
-  } else if (W == 5) {
-    const double sum = 2.0 * (v[0] / s) - 13.0 * (v[1] / s) + 47.0 * (v[2] / s) +
-                       27.0 * (v[3] / s) - 3.0 * (v[4] / s);
-    vl = (sum / 60.0) * s;
   } else {
-    const double sum = -3.0 * (v[0] / s) + 25.0 * (v[1] / s) - 101.0 * (v[2] / s) +
-                       319.0 * (v[3] / s) + 214.0 * (v[4] / s) - 38.0 * (v[5] / s) +
-                       4.0 * (v[6] / s);
-    vl = (sum / 420.0) * s;
+    const double is = 1.0 / s;
+    if (W == 5) {
+      const double sum = 2.0 * (v[0] * is) - 13.0 * (v[1] * is) + 47.0 * (v[2] * is) +
+                         27.0 * (v[3] * is) - 3.0 * (v[4] * is);
+      vl = (sum / 60.0) * s;
+    } else {
+      const double sum = -3.0 * (v[0] * is) + 25.0 * (v[1] * is) - 101.0 * (v[2] * is) +
+                         319.0 * (v[3] * is) + 214.0 * (v[4] * is) - 38.0 * (v[5] * is) +
+                         4.0 * (v[6] * is);
+      vl = (sum / 420.0) * s;
+    }
   }
   constexpr int o = W == 5 ? 0 : 1;
   return mp_limit(vl, v[o], v[o + 1], v[o + 2], v[o + 3], v[o + 4], fired);
 }
 
 // ---- HLLD: numerics/hlld_core.hpp ----------------------------------------
-// hlld_core.hpp:123-153
-__device__ __forceinline__ Fx physical_flux_x(const St& u, double gamma) {
-  const double vx = u.mx / u.rho, vy = u.my / u.rho, vz = u.mz / u.rho;
-  const double p = pressure(u, gamma);
-  const double hbn = half_sq3(u.bx, 0.0, 0.0);
-  const double hbt = half_sq3(0.0, u.by, u.bz);
+// hlld_core.hpp:123-153, from the state, its pressure and 1/rho
+__device__ __forceinline__ Fx physical_flux_xp(const St& u, double p, double ir) {
+  const double vx = u.mx * ir, vy = u.my * ir, vz = u.mz * ir;
+  const double hbn = 0.5 * (u.bx * u.bx);
+  const double hbt = 0.5 * (u.by * u.by + u.bz * u.bz);
   Fx f;
   f.rho = u.mx;
   f.mx = u.mx * vx + p + u.by * (0.5 * u.by) + u.bz * (0.5 * u.bz) + u.bx * (-0.5 * u.bx);
@@ -288,6 +320,10 @@ __device__ __forceinline__ Fx physical_flux_x(const St& u, double gamma) {
   f.by = u.by * vx + u.bx * (-vy);
   f.bz = u.bz * vx + u.bx * (-vz);
   return f;
+}
+__device__ __forceinline__ Fx physical_flux_x(const St& u, double gamma) {
+  const double ir = 1.0 / u.rho;
+  return physical_flux_xp(u, pressure_f(u, gamma, ir), ir);
 }
 __device__ __forceinline__ bool flux_finite(const Fx& f) {
   return isfinite(f.rho) && isfinite(f.mx) && isfinite(f.my) && isfinite(f.mz) &&
@@ -320,8 +356,9 @@ __device__ __noinline__ Fx hll_flux_x(const St& L, const St& R, double sl, doubl
 }
 // hlld_core.hpp:200-210
 __device__ __forceinline__ Fx lf_flux_x(const St& L, const St& R, double gamma) {
-  const double aL = fabs(L.mx / L.rho) + fast_x(L, gamma);
-  const double aR = fabs(R.mx / R.rho) + fast_x(R, gamma);
+  const double irl = 1.0 / L.rho, irr = 1.0 / R.rho;
+  const double aL = fabs(L.mx * irl) + fast_x_f(L, pressure_f(L, gamma, irl), irl, gamma);
+  const double aR = fabs(R.mx * irr) + fast_x_f(R, pressure_f(R, gamma, irr), irr, gamma);
   const double a = (aL > aR) ? aL : aR;
   return hll_flux_x(L, R, -a, a, gamma);
 }
@@ -331,14 +368,14 @@ __device__ __forceinline__ bool same_state(const St& a, const St& b) {
 }
 
 // hlld_core.hpp:213-457 (B0 inactive).
-__device__ __noinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double gamma) {
+__device__ __forceinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double gamma) {
   const double rel = 64.0 * kEps;
   if (same_state(Lin, Rin)) return physical_flux_x(Lin, gamma);
   const double bn = 0.5 * Lin.bx + 0.5 * Rin.bx;
   St L = Lin, R = Rin;
-  const double hbn2 = half_sq3(bn, 0.0, 0.0);
-  L.E = (L.E - half_sq3(L.bx, 0.0, 0.0)) + hbn2;
-  R.E = (R.E - half_sq3(R.bx, 0.0, 0.0)) + hbn2;
+  const double hbn2 = 0.5 * (bn * bn);
+  L.E = (L.E - 0.5 * (L.bx * L.bx)) + hbn2;
+  R.E = (R.E - 0.5 * (R.bx * R.bx)) + hbn2;
   L.bx = bn;
   R.bx = bn;
   const bool bn2_ok = hbn2 <= 0.5 * 1.7976931348623157e308;
@@ -346,15 +383,15 @@ __device__ __noinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double gamm
   const double irl = 1.0 / L.rho, irr = 1.0 / R.rho;
   const double vxL = L.mx * irl, vyL = L.my * irl, vzL = L.mz * irl;
   const double vxR = R.mx * irr, vyR = R.my * irr, vzR = R.mz * irr;
-  const double pL = pressure(L, gamma), pR = pressure(R, gamma);
-  const double ptL = pL + half_sq3(L.bx, L.by, L.bz);
-  const double ptR = pR + half_sq3(R.bx, R.by, R.bz);
-  const double cfL = fast_x(L, gamma), cfR = fast_x(R, gamma);
+  const double pL = pressure_f(L, gamma, irl), pR = pressure_f(R, gamma, irr);
+  const double ptL = pL + 0.5 * (L.bx * L.bx + L.by * L.by + L.bz * L.bz);
+  const double ptR = pR + 0.5 * (R.bx * R.bx + R.by * R.by + R.bz * R.bz);
+  const double cfL = fast_x_f(L, pL, irl, gamma), cfR = fast_x_f(R, pR, irr, gamma);
   const double cfm = (cfL > cfR) ? cfL : cfR;
   const double sl = ((vxL < vxR) ? vxL : vxR) - cfm;
   const double sr = ((vxL > vxR) ? vxL : vxR) + cfm;
-  if (sl >= 0.0) return physical_flux_x(L, gamma);
-  if (sr <= 0.0) return physical_flux_x(R, gamma);
+  if (sl >= 0.0) return physical_flux_xp(L, pL, irl);
+  if (sr <= 0.0) return physical_flux_xp(R, pR, irr);
   if (!bn2_ok || !isfinite(ptL) || !isfinite(ptR)) return hll_flux_x(L, R, sl, sr, gamma);
   auto resolved = [&](double v, double s) { return isfinite(v) && fabs(v) > rel * (s + kTiny); };
   const double aR = (sr - vxR) * R.rho, aL = (sl - vxL) * L.rho;
@@ -410,6 +447,8 @@ __device__ __noinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double gamm
   const double sqL = sqrt(rhoLs), sqR = sqrt(rhoRs);
   const double saL = sm - fabs(bn) / sqL;
   const double saR = sm + fabs(bn) / sqR;
+  // (the reference forms both; only the upwind side's single-star state is
+  // needed below, the other enters the double-star average)
   const bool negl = bn2 <= rel * (fabs(pts) + fabs(ptL) + fabs(ptR) + kTiny);
   auto star_flux = [&](const St& U, const St& us, double s, double f_rho, double f_mx,
                        double f_my, double f_mz, double f_E, double f_by, double f_bz) {
@@ -426,7 +465,7 @@ __device__ __noinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double gamm
   };
   const bool left_side = negl ? (sl <= 0.0 && 0.0 <= sm) : (0.0 <= sm);
   const St& U = left_side ? L : R;
-  const Fx fU = physical_flux_x(U, gamma);
+  const Fx fU = left_side ? physical_flux_xp(L, pL, irl) : physical_flux_xp(R, pR, irr);
   if (negl) {
     const Fx f = left_side ? star_flux(L, usL, sl, fU.rho, fU.mx, fU.my, fU.mz, fU.E, fU.by, fU.bz)
                            : star_flux(R, usR, sr, fU.rho, fU.mx, fU.my, fU.mz, fU.E, fU.by, fU.bz);

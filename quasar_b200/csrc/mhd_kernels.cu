@@ -322,147 +322,145 @@ __device__ __forceinline__ void set_normal_b(St& s, double v) {
   bn = v;
 }
 
-// Conserved-variable 7-wave eigenvectors about `s` (x-normal), built as
-// L = Lp dW/dU and R = dU/dW Rp with the reference's biorthogonality
-// fallback to the identity (numerics/mhd_eigensystem.hpp:58-431).
-// L row-major (waves x vars), R stored R[var*7 + wave].
-__device__ void build_eig(const St& s, double gamma, double* L, double* R) {
+// ---- characteristic eigensystem, one wave at a time ----------------------
+// Scalars of the eigensystem about a canonical (x-normal) state
+// (mhd_eigensystem.hpp:63-171), shared by all seven waves.
+struct Eg {
+  double rho, sr, cf, cs, a, af, as, b1, b2, sbn, vn, vt1, vt2, bt1, bt2;
+  double ia2, ra2, gm1, hv2, ir;
+};
+
+__device__ __forceinline__ Eg eig_scalars(const St& s, double gamma) {
+  Eg e;
   const Pr w = to_prim(s, gamma);
-  const double rho = w.rho;
+  e.rho = w.rho;
   const double p = w.p > 0.0 ? w.p : 0.0;
-  const double sr = sqrt(rho);
-  const double bn = w.bx, bt1 = w.by, bt2 = w.bz;
-  double cf, cs, a, cax, ca;
-  magnetosonic(rho, p, bn, bt1, bt2, gamma, cf, cs, a, cax, ca);
-  double af, as;
+  e.sr = sqrt(e.rho);
+  e.bt1 = w.by;
+  e.bt2 = w.bz;
+  double cax, ca;
+  magnetosonic(e.rho, p, w.bx, w.by, w.bz, gamma, e.cf, e.cs, e.a, cax, ca);
   {
-    // contraction-free: af2/as2 are differences of nearly equal squares at a
-    // degenerate fan (mhd_eigensystem.hpp:91-110)
-    const double sc = cf > 0.0 ? cf : 1.0;
-    const double cfn = cf / sc, csn = cs / sc, an = a / sc;
+    const double sc = e.cf > 0.0 ? e.cf : 1.0;
+    const double cfn = e.cf / sc, csn = e.cs / sc, an = e.a / sc;
     const double den = sub(mul(cfn, cfn), mul(csn, csn));
     if (den <= mul(64.0 * kEps, add(mul(cfn, cfn), mul(csn, csn)))) {
-      af = 1.0 / sqrt(2.0);
-      as = 1.0 / sqrt(2.0);
+      e.af = 1.0 / sqrt(2.0);
+      e.as = 1.0 / sqrt(2.0);
     } else {
-      double af2 = sub(mul(an, an), mul(csn, csn)) / den;
-      double as2 = sub(mul(cfn, cfn), mul(an, an)) / den;
-      af = sqrt(af2 < 0.0 ? 0.0 : af2);
-      as = sqrt(as2 < 0.0 ? 0.0 : as2);
+      const double af2 = sub(mul(an, an), mul(csn, csn)) / den;
+      const double as2 = sub(mul(cfn, cfn), mul(an, an)) / den;
+      e.af = sqrt(af2 < 0.0 ? 0.0 : af2);
+      e.as = sqrt(as2 < 0.0 ? 0.0 : as2);
     }
   }
-  double b1, b2;
   {
-    const double bt = scaled_norm3(bt1, bt2, 0.0);
-    const double fs = a > ca ? a : ca;
-    if (bt == 0.0 || bt / sr <= 64.0 * kEps * (fs + kTiny)) {
-      b1 = 1.0 / sqrt(2.0);
-      b2 = 1.0 / sqrt(2.0);
+    const double bt = scaled_norm3(w.by, w.bz, 0.0);
+    const double fs = e.a > ca ? e.a : ca;
+    if (bt == 0.0 || bt / e.sr <= 64.0 * kEps * (fs + kTiny)) {
+      e.b1 = 1.0 / sqrt(2.0);
+      e.b2 = 1.0 / sqrt(2.0);
     } else {
-      b1 = bt1 / bt;
-      b2 = bt2 / bt;
+      e.b1 = w.by / bt;
+      e.b2 = w.bz / bt;
     }
   }
-  const double sbn = bn >= 0.0 ? 1.0 : -1.0;
-  const double vn = w.vx, vt1 = w.vy, vt2 = w.vz;
-  const double qf = cf * af * sbn, qs = cs * as * sbn;
-  const double Af = a * af * sr, As = a * as * sr;
-  const double ia2 = a > 0.0 ? (1.0 / a) / a : 0.0;
-  const double Nf = 0.5 * ia2;
-  const double ra2 = gamma * p;
-  const double s2 = 1.0 / sqrt(2.0);
-  double Rp[7][7], Lp[7][7];
+  e.sbn = w.bx >= 0.0 ? 1.0 : -1.0;
+  e.vn = w.vx;
+  e.vt1 = w.vy;
+  e.vt2 = w.vz;
+  e.ia2 = e.a > 0.0 ? (1.0 / e.a) / e.a : 0.0;
+  e.ra2 = gamma * p;
+  e.gm1 = gamma - 1.0;
+  e.hv2 = half_sq3(e.vn, e.vt1, e.vt2);
+  e.ir = 1.0 / e.rho;
+  return e;
+}
+
+// Primitive left row and right column of wave k (mhd_eigensystem.hpp:176-320);
+// k = 7 (the spare lane) gets zeros.
+__device__ __forceinline__ void wave_vectors(const Eg& e, int k, double* lp, double* rp) {
 #pragma unroll
-  for (int k = 0; k < 7; ++k)
-#pragma unroll
-    for (int v = 0; v < 7; ++v) {
-      Rp[k][v] = 0.0;
-      Lp[k][v] = 0.0;
-    }
-  Rp[0][0] = rho * af; Rp[0][1] = -af * cf; Rp[0][2] = qs * b1; Rp[0][3] = qs * b2;
-  Rp[0][4] = af * ra2; Rp[0][5] = As * b1; Rp[0][6] = As * b2;
-  Rp[6][0] = rho * af; Rp[6][1] = af * cf; Rp[6][2] = -qs * b1; Rp[6][3] = -qs * b2;
-  Rp[6][4] = af * ra2; Rp[6][5] = As * b1; Rp[6][6] = As * b2;
-  Rp[1][2] = -b2 * s2; Rp[1][3] = b1 * s2;
-  Rp[1][5] = -sbn * b2 * s2 * sr; Rp[1][6] = sbn * b1 * s2 * sr;
-  Rp[5][2] = -b2 * s2; Rp[5][3] = b1 * s2;
-  Rp[5][5] = sbn * b2 * s2 * sr; Rp[5][6] = -sbn * b1 * s2 * sr;
-  Rp[2][0] = rho * as; Rp[2][1] = -as * cs; Rp[2][2] = -qf * b1; Rp[2][3] = -qf * b2;
-  Rp[2][4] = as * ra2; Rp[2][5] = -Af * b1; Rp[2][6] = -Af * b2;
-  Rp[4][0] = rho * as; Rp[4][1] = as * cs; Rp[4][2] = qf * b1; Rp[4][3] = qf * b2;
-  Rp[4][4] = as * ra2; Rp[4][5] = -Af * b1; Rp[4][6] = -Af * b2;
-  Rp[3][0] = 1.0;
-  Lp[0][1] = -Nf * af * cf; Lp[0][2] = Nf * qs * b1; Lp[0][3] = Nf * qs * b2;
-  Lp[0][4] = Nf * af / rho; Lp[0][5] = Nf * As * b1 / rho; Lp[0][6] = Nf * As * b2 / rho;
-  Lp[6][1] = Nf * af * cf; Lp[6][2] = -Nf * qs * b1; Lp[6][3] = -Nf * qs * b2;
-  Lp[6][4] = Nf * af / rho; Lp[6][5] = Nf * As * b1 / rho; Lp[6][6] = Nf * As * b2 / rho;
-  Lp[1][2] = -b2 * s2; Lp[1][3] = b1 * s2;
-  Lp[1][5] = -sbn * b2 * s2 / sr; Lp[1][6] = sbn * b1 * s2 / sr;
-  Lp[5][2] = -b2 * s2; Lp[5][3] = b1 * s2;
-  Lp[5][5] = sbn * b2 * s2 / sr; Lp[5][6] = -sbn * b1 * s2 / sr;
-  Lp[2][1] = -Nf * as * cs; Lp[2][2] = -Nf * qf * b1; Lp[2][3] = -Nf * qf * b2;
-  Lp[2][4] = Nf * as / rho; Lp[2][5] = -Nf * Af * b1 / rho; Lp[2][6] = -Nf * Af * b2 / rho;
-  Lp[4][1] = Nf * as * cs; Lp[4][2] = Nf * qf * b1; Lp[4][3] = Nf * qf * b2;
-  Lp[4][4] = Nf * as / rho; Lp[4][5] = -Nf * Af * b1 / rho; Lp[4][6] = -Nf * Af * b2 / rho;
-  Lp[3][0] = 1.0; Lp[3][4] = -ia2;
-  // M = dU/dW and its analytic inverse, written as their non-zero pattern.
-  const double gm1 = gamma - 1.0;
-  const double hv2 = half_sq3(vn, vt1, vt2);
-  const double ir = 1.0 / rho;
-  const double Mi0[5] = {1.0, -vn * ir, -vt1 * ir, -vt2 * ir, gm1 * hv2};  // column 0, rows 0..4
-  const double Mi4[7] = {gm1 * hv2, -gm1 * vn, -gm1 * vt1, -gm1 * vt2, gm1, -gm1 * bt1, -gm1 * bt2};
-  const double Mdiag[7] = {1.0, ir, ir, ir, gm1, 1.0, 1.0};
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    // L[k][v] = sum_j Lp[k][j] Minv[j][v]   (j ascending, zeros skipped)
-    double l0 = 0.0;
-#pragma unroll
-    for (int j = 0; j < 5; ++j) l0 += Lp[k][j] * Mi0[j];
-    L[k * 7 + 0] = l0;
-#pragma unroll
-    for (int v = 1; v < 7; ++v) {
-      double acc = Lp[k][v] * (v == 4 ? Mi4[4] : Mdiag[v]);
-      if (v < 4) acc = acc + Lp[k][4] * Mi4[v];
-      if (v > 4) acc = Lp[k][4] * Mi4[v] + Lp[k][v] * Mdiag[v];
-      L[k * 7 + v] = acc;
-    }
-    // R[v][k] = sum_j M[v][j] Rp[k][j]
-    R[0 * 7 + k] = Rp[k][0];
-    R[1 * 7 + k] = vn * Rp[k][0] + rho * Rp[k][1];
-    R[2 * 7 + k] = vt1 * Rp[k][0] + rho * Rp[k][2];
-    R[3 * 7 + k] = vt2 * Rp[k][0] + rho * Rp[k][3];
-    R[4 * 7 + k] = (((((hv2 * Rp[k][0] + (rho * vn) * Rp[k][1]) + (rho * vt1) * Rp[k][2]) +
-                      (rho * vt2) * Rp[k][3]) + (1.0 / gm1) * Rp[k][4]) + bt1 * Rp[k][5]) +
-                   bt2 * Rp[k][6];
-    R[5 * 7 + k] = Rp[k][5];
-    R[6 * 7 + k] = Rp[k][6];
+  for (int v = 0; v < 7; ++v) {
+    lp[v] = 0.0;
+    rp[v] = 0.0;
   }
-  bool usable = true;
-  for (int i = 0; i < 7 && usable; ++i)
-    for (int jj = 0; jj < 7; ++jj) {
-      double dot = 0.0;
-#pragma unroll
-      for (int k = 0; k < 7; ++k) dot += L[i * 7 + k] * R[k * 7 + jj];
-      const double expect = i == jj ? 1.0 : 0.0;
-      if (!isfinite(dot) || fabs(dot - expect) > 1024.0 * kEps) {
-        usable = false;
-        break;
-      }
-    }
-  if (!usable) {
-#pragma unroll
-    for (int e = 0; e < 49; ++e) {
-      L[e] = (e % 8 == 0) ? 1.0 : 0.0;
-      R[e] = (e % 8 == 0) ? 1.0 : 0.0;
-    }
+  const double rho = e.rho;
+  const double qf = e.cf * e.af * e.sbn, qs = e.cs * e.as * e.sbn;
+  const double Af = e.a * e.af * e.sr, As = e.a * e.as * e.sr;
+  const double Nf = 0.5 * e.ia2, s2 = 1.0 / sqrt(2.0);
+  if (k == 0 || k == 6) {
+    rp[0] = rho * e.af;
+    rp[1] = k == 0 ? -e.af * e.cf : e.af * e.cf;
+    rp[2] = k == 0 ? qs * e.b1 : -qs * e.b1;
+    rp[3] = k == 0 ? qs * e.b2 : -qs * e.b2;
+    rp[4] = e.af * e.ra2;
+    rp[5] = As * e.b1;
+    rp[6] = As * e.b2;
+    lp[1] = k == 0 ? -Nf * e.af * e.cf : Nf * e.af * e.cf;
+    lp[2] = k == 0 ? Nf * qs * e.b1 : -Nf * qs * e.b1;
+    lp[3] = k == 0 ? Nf * qs * e.b2 : -Nf * qs * e.b2;
+    lp[4] = Nf * e.af / rho;
+    lp[5] = Nf * As * e.b1 / rho;
+    lp[6] = Nf * As * e.b2 / rho;
+  } else if (k == 1 || k == 5) {
+    rp[2] = -e.b2 * s2;
+    rp[3] = e.b1 * s2;
+    rp[5] = k == 1 ? -e.sbn * e.b2 * s2 * e.sr : e.sbn * e.b2 * s2 * e.sr;
+    rp[6] = k == 1 ? e.sbn * e.b1 * s2 * e.sr : -e.sbn * e.b1 * s2 * e.sr;
+    lp[2] = -e.b2 * s2;
+    lp[3] = e.b1 * s2;
+    lp[5] = k == 1 ? -e.sbn * e.b2 * s2 / e.sr : e.sbn * e.b2 * s2 / e.sr;
+    lp[6] = k == 1 ? e.sbn * e.b1 * s2 / e.sr : -e.sbn * e.b1 * s2 / e.sr;
+  } else if (k == 2 || k == 4) {
+    rp[0] = rho * e.as;
+    rp[1] = k == 2 ? -e.as * e.cs : e.as * e.cs;
+    rp[2] = k == 2 ? -qf * e.b1 : qf * e.b1;
+    rp[3] = k == 2 ? -qf * e.b2 : qf * e.b2;
+    rp[4] = e.as * e.ra2;
+    rp[5] = -Af * e.b1;
+    rp[6] = -Af * e.b2;
+    lp[1] = k == 2 ? -Nf * e.as * e.cs : Nf * e.as * e.cs;
+    lp[2] = k == 2 ? -Nf * qf * e.b1 : Nf * qf * e.b1;
+    lp[3] = k == 2 ? -Nf * qf * e.b2 : Nf * qf * e.b2;
+    lp[4] = Nf * e.as / rho;
+    lp[5] = -Nf * Af * e.b1 / rho;
+    lp[6] = -Nf * Af * e.b2 / rho;
+  } else if (k == 3) {
+    rp[0] = 1.0;
+    lp[0] = 1.0;
+    lp[4] = -e.ia2;
   }
 }
 
-// MP5 (H=2) / MP7 (H=3) characteristic L and R states at the face between
-// cells k0-step and k0 (mhd_reconstruct.hip:217-349, 525-616).
+// One thread per face, wave loop rolled: L row and R column of each wave are
+// rebuilt from the shared eigen scalars when needed, so only the stencil
+// deltas stay resident.  Same arithmetic per entry as build_eig.
+__device__ __forceinline__ void conserved_row_col(const Eg& e, int k, double* Lr, double* Rc) {
+  double lp[7], rp[7];
+  wave_vectors(e, k, lp, rp);
+  const double gv = e.gm1;
+  Lr[0] = (((lp[0] * 1.0 + lp[1] * (-e.vn * e.ir)) + lp[2] * (-e.vt1 * e.ir)) +
+           lp[3] * (-e.vt2 * e.ir)) + lp[4] * (gv * e.hv2);
+  Lr[1] = lp[1] * e.ir + lp[4] * (-gv * e.vn);
+  Lr[2] = lp[2] * e.ir + lp[4] * (-gv * e.vt1);
+  Lr[3] = lp[3] * e.ir + lp[4] * (-gv * e.vt2);
+  Lr[4] = lp[4] * gv;
+  Lr[5] = lp[4] * (-gv * e.bt1) + lp[5];
+  Lr[6] = lp[4] * (-gv * e.bt2) + lp[6];
+  Rc[0] = rp[0];
+  Rc[1] = e.vn * rp[0] + e.rho * rp[1];
+  Rc[2] = e.vt1 * rp[0] + e.rho * rp[2];
+  Rc[3] = e.vt2 * rp[0] + e.rho * rp[3];
+  Rc[4] = (((((e.hv2 * rp[0] + (e.rho * e.vn) * rp[1]) + (e.rho * e.vt1) * rp[2]) +
+             (e.rho * e.vt2) * rp[3]) + (1.0 / gv) * rp[4]) + e.bt1 * rp[5]) + e.bt2 * rp[6];
+  Rc[5] = rp[5];
+  Rc[6] = rp[6];
+}
+
 template <int DIR, int H>
-__device__ void mp_pair(const StateP& u, long long k0, long long step, double gamma, St& ul,
-                        St& ur) {
+__device__ void mp_pair_loop(const StateP& u, long long k0, long long step, double gamma, St& ul,
+                             St& ur) {
   constexpr int S = 2 * H + 2, W = 2 * H + 1;
   const St cl = load_cell(u, k0 - step), cr = load_cell(u, k0);
   St ref;
@@ -475,21 +473,43 @@ __device__ void mp_pair(const StateP& u, long long k0, long long step, double ga
   ref.by = 0.5 * cl.by + 0.5 * cr.by;
   ref.bz = 0.5 * cl.bz + 0.5 * cr.bz;
   const St c = rot<DIR>(ref);
-  double L[49], R[49];
-  build_eig(c, gamma, L, R);
-  double ch[S][7];
+  const Eg e = eig_scalars(c, gamma);
+  // L R = I check (mhd_eigensystem.hpp:416-430): all R columns resident,
+  // L rows one at a time
+  bool usable = true;
+  {
+    double R[7][7];
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      double Lr[7];
+      conserved_row_col(e, j, Lr, R[j]);
+    }
+#pragma unroll 1
+    for (int i = 0; i < 7; ++i) {
+      double Lr[7], Rc[7];
+      conserved_row_col(e, i, Lr, Rc);
+#pragma unroll
+      for (int j = 0; j < 7; ++j) {
+        double dot = 0.0;
+#pragma unroll
+        for (int m = 0; m < 7; ++m) dot += Lr[m] * R[j][m];
+        const double expect = i == j ? 1.0 : 0.0;
+        if (!isfinite(dot) || fabs(dot - expect) > 1024.0 * kEps) usable = false;
+      }
+    }
+  }
+  // stencil deltas in the canonical frame
+  double u7[S][7];
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const St d = rot<DIR>(load_cell(u, k0 + (long long)(s - 1 - H) * step));
-    const double u7[7] = {d.rho - c.rho, d.mx - c.mx, d.my - c.my, d.mz - c.mz,
-                          d.E - c.E,     d.by - c.by, d.bz - c.bz};
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      double acc = 0.0;
-#pragma unroll
-      for (int v = 0; v < 7; ++v) acc += L[k * 7 + v] * u7[v];
-      ch[s][k] = acc;
-    }
+    u7[s][0] = d.rho - c.rho;
+    u7[s][1] = d.mx - c.mx;
+    u7[s][2] = d.my - c.my;
+    u7[s][3] = d.mz - c.mz;
+    u7[s][4] = d.E - c.E;
+    u7[s][5] = d.by - c.by;
+    u7[s][6] = d.bz - c.bz;
   }
   double dl[7], dr[7];
 #pragma unroll
@@ -497,20 +517,38 @@ __device__ void mp_pair(const StateP& u, long long k0, long long step, double ga
     dl[v] = 0.0;
     dr[v] = 0.0;
   }
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < 7; ++k) {
+    double Lr[7], Rc[7];
+    if (usable) {
+      conserved_row_col(e, k, Lr, Rc);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 7; ++v) {
+        Lr[v] = v == k ? 1.0 : 0.0;
+        Rc[v] = v == k ? 1.0 : 0.0;
+      }
+    }
+    double ch[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      double acc = 0.0;
+#pragma unroll
+      for (int v = 0; v < 7; ++v) acc += Lr[v] * u7[s][v];
+      ch[s] = acc;
+    }
     double win[W];
     bool f;
 #pragma unroll
-    for (int s = 0; s < W; ++s) win[s] = ch[s][k];
+    for (int s = 0; s < W; ++s) win[s] = ch[s];
     const double wl = mp_recon<W>(win, f);
 #pragma unroll
-    for (int s = 0; s < W; ++s) win[s] = ch[W - s][k];
+    for (int s = 0; s < W; ++s) win[s] = ch[W - s];
     const double wr = mp_recon<W>(win, f);
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
-      dl[v] += R[v * 7 + k] * wl;
-      dr[v] += R[v * 7 + k] * wr;
+      dl[v] += Rc[v] * wl;
+      dr[v] += Rc[v] * wr;
     }
   }
   const St sl{c.rho + dl[0], c.mx + dl[1], c.my + dl[2], c.mz + dl[3],
@@ -577,7 +615,7 @@ __global__ void __launch_bounds__(128) k_reconstruct(Grid g, StateP u, IfaceP ou
   } else if (ORDER == 2) {
     muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
   } else {
-    mp_pair<DIR, ORDER == 5 ? 2 : 3>(u, k0, step, gamma, ul, ur);
+    mp_pair_loop<DIR, ORDER == 5 ? 2 : 3>(u, k0, step, gamma, ul, ur);
     if (!recon_admissible(ul, gamma) || !recon_admissible(ur, gamma))
       muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
   }
@@ -607,6 +645,7 @@ __global__ void __launch_bounds__(128) k_reconstruct(Grid g, StateP u, IfaceP ou
   }
 }
 
+
 }  // namespace
 
 // ===========================================================================
@@ -620,7 +659,10 @@ struct Spd {
   double v, f;
 };
 
-// One side's |v_n| and fast speed (mhd_reduce.hip:254-325).
+// One side's |v_n| and fast speed (mhd_reduce.hip:254-325).  Kept in the
+// reference's scaled form: dt is the max of these and, at a degenerate fan
+// (a^2 == b_n^2, b_t == 0), the discriminant's rounding is amplified to
+// sqrt(eps), so any reassociation moves dt by ~1e-9.
 template <int DIR>
 __device__ Spd speed_parts(const St& s, double gamma) {
   const double p = pressure(s, gamma);
@@ -779,6 +821,120 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// MP5/MP7 face flux with one lane per Gauss point: a group of four lanes owns
+// a face (eight faces per warp).  Each lane recovers its point state and
+// solves its Riemann problem; the group votes on admissibility, gathers the
+// point fluxes in node order for the Gauss sum, and splits the stores.
+// Same arithmetic as k_face_flux (node order of every sum kept).
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128) k_face_flux_q(Grid g, IfaceP in, FluxP out, double* emf,
+                                                     int* nj, double* spd, double gamma,
+                                                     const Ctl* ctl) {
+  constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
+  constexpr bool kLF = false;
+  const int lane = threadIdx.x & 3;
+  const unsigned gmask = 0xFu << (threadIdx.x & 28);
+  const int i = blockIdx.x * 32 + (threadIdx.x >> 2);
+  const int j = blockIdx.y;
+  if (i > g.nx || j > g.ny) return;  // whole four-lane groups leave together
+  if (ctl->status) return;
+  int si = i, sj = j;
+  if (DIR == 0 && i == g.nx && g.bc[0] == 0 && g.bc[1] == 0) si = 0;
+  if (DIR == 1 && j == g.ny && g.bc[2] == 0 && g.bc[3] == 0) sj = 0;
+  const long long k = g.idx(i, j), ks = g.idx(si, sj);
+  const double h = DIR == 0 ? g.dx : g.dy;
+  const long long ts = DIR == 0 ? g.pitch : 1;
+  // this lane's Gauss node (lanes >= Q only help with the base problem)
+  St l{}, r{};
+  bool ok = true;
+  if (lane < Q) {
+    double w[N];
+#pragma unroll
+    for (int t = 0; t < N; ++t) w[t] = point_w<ORDER>(lane, t);
+    double pl[8], pr[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      double sa[N], sb[N];
+#pragma unroll
+      for (int t = 0; t < N; ++t) {
+        sa[t] = __ldg(in.L[c] + ks + (t - H) * ts);
+        sb[t] = __ldg(in.R[c] + ks + (t - H) * ts);
+      }
+      pl[c] = wsum<N>(w, sa);
+      pr[c] = wsum<N>(w, sb);
+    }
+    l = St{pl[0], pl[1], pl[2], pl[3], pl[4], pl[5], pl[6], pl[7]};
+    r = St{pr[0], pr[1], pr[2], pr[3], pr[4], pr[5], pr[6], pr[7]};
+    ok = point_admissible(l, gamma) && point_admissible(r, gamma);
+  }
+  const unsigned bad = (__ballot_sync(gmask, !ok) >> (threadIdx.x & 28)) & 0xFu;
+  const bool group_ok = bad == 0;
+  const int first_bad = bad ? __ffs(bad) - 1 : Q;
+  double rate = 0.0;
+  if (spd) {
+    if (lane == 0) rate = face_rate<DIR, ORDER>(iface(in, ks, true), iface(in, ks, false), gamma, h);
+    if (lane < first_bad) rate = fmax(rate, face_rate<DIR, ORDER>(l, r, gamma, h));
+  }
+  // one Riemann solve per lane: its point, or (fallback) the face average
+  const bool solve = group_ok ? lane < Q : lane == 0;
+  if (!group_ok) {
+    l = iface(in, ks, true);
+    r = iface(in, ks, false);
+  }
+  double fv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (solve) {
+    const Fx f = riemann<DIR>(l, r, kLF, gamma);
+    fv[0] = f.rho; fv[1] = f.mx; fv[2] = f.my; fv[3] = f.mz;
+    fv[4] = f.E;   fv[5] = f.bx; fv[6] = f.by; fv[7] = f.bz;
+  }
+  double res[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    if (group_ok) {
+      double sq[Q];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) sq[q] = __shfl_sync(gmask, fv[c], q, 4);
+      res[c] = gauss_avg<ORDER>(sq);
+    } else {
+      res[c] = __shfl_sync(gmask, fv[c], 0, 4);
+    }
+  }
+  // stores split over the group: lane q writes components q and q+4
+  const double lo = lane == 0 ? res[0] : lane == 1 ? res[1] : lane == 2 ? res[2] : res[3];
+  const double hi = lane == 0 ? res[4] : lane == 1 ? res[5] : lane == 2 ? res[6] : res[7];
+  out.f[lane][k] = lo;
+  out.f[lane + 4][k] = hi;
+  if (lane == 0) emf[k] = DIR == 0 ? -res[6] : res[5];
+  if (spd) {
+    rate = fmax(rate, __shfl_xor_sync(gmask, rate, 1, 4));
+    rate = fmax(rate, __shfl_xor_sync(gmask, rate, 2, 4));
+    if (lane == 0) spd[k] = rate;
+  }
+  // no-jump proof over the 2H+1 transverse taps, split across the group
+  constexpr int RH = H;
+  int proof = 1;
+  for (int off = lane - RH; off <= RH; off += 4) {
+    const int mi = face_index(DIR == 0 ? i : i + off, g.nx, g.bc[0], g.bc[1]);
+    const int mj = face_index(DIR == 0 ? j + off : j, g.ny, g.bc[2], g.bc[3]);
+    if (!in_pad(g, mi, mj)) {
+      proof = 0;
+      break;
+    }
+    const long long km = g.idx(mi, mj);
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (!(in.L[c][km] == in.R[c][km])) proof = 0;
+  }
+  const unsigned nproof = (__ballot_sync(gmask, proof == 0) >> (threadIdx.x & 28)) & 0xFu;
+  if (lane == 0) nj[k] = nproof == 0 ? 1 : 0;
+}
+
+}  // namespace
+
 // ===========================================================================
 // Constrained transport and the stage update
 // ===========================================================================
@@ -866,6 +1022,116 @@ __global__ void __launch_bounds__(128) k_cell_emf(Grid g, StateP u, double* cell
   if (tid == 0) {
     double m = s_max[0];
     for (int w = 1; w < (int)(blockDim.x * blockDim.y + 31) / 32; ++w) m = fmax(m, s_max[w]);
+    atomicMax(&ctl->max_rate, dbits(m));
+  }
+}
+
+// Tiled form of k_cell_emf for MP5/MP7: a 32x8 tile of cells and its
+// H-wide halo are staged in shared memory once; for each x-node the
+// x-recovered rows of the tile (all 8 components) are formed once in shared
+// memory and every cell then recovers its y-nodes from them.  Same sums in
+// the same order as k_cell_emf.
+constexpr int kCellTX = 32, kCellTY = 8;
+
+template <int ORDER>
+constexpr int cell_smem_doubles() {
+  return 8 * (kCellTY + 2 * (ORDER == 7 ? 3 : 2)) *
+         ((kCellTX + 2 * (ORDER == 7 ? 3 : 2)) + kCellTX);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(256) k_cell_emf_s(Grid g, StateP u, double* cell_ez,
+                                                    const double* xs, const double* ys,
+                                                    int cfl_reduce, double gamma, Ctl* ctl) {
+  constexpr int H = ORDER == 7 ? 3 : 2, N = 2 * H + 1, Q = ORDER == 7 ? 4 : 3;
+  constexpr int TX = kCellTX, TY = kCellTY, SX = TX + 2 * H, SY = TY + 2 * H;
+  extern __shared__ double sm[];
+  double* S = sm;                // [8][SY][SX] staged state
+  double* X = sm + 8 * SY * SX;  // [8][SY][TX] x-recovered rows of one x-node
+  __shared__ int s_stop;
+  __shared__ double s_max[8];
+  const int tid = threadIdx.y * TX + threadIdx.x;
+  if (tid == 0) s_stop = ctl->status;
+  __syncthreads();
+  if (s_stop) return;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const double* src = c < 5 ? u.c[c] : c == 5 ? u.bxc : c == 6 ? u.byc : u.c[7];
+    for (int e = tid; e < SY * SX; e += TX * TY) {
+      const int r = e / SX, x = e - r * SX;
+      const int ii = i0 - H + x, jj = j0 - H + r;
+      S[c * SY * SX + e] = in_pad(g, ii, jj) ? __ldg(src + g.idx(ii, jj)) : 0.0;
+    }
+  }
+  __syncthreads();
+  const bool phx = g.bc[1] != 0, phy = g.bc[3] != 0;
+  const bool active =
+      i <= g.nx && j <= g.ny && !((i == g.nx && !phx) || (j == g.ny && !phy));
+  double pt[Q][Q];
+  bool ok = true;
+#pragma unroll
+  for (int qx = 0; qx < Q; ++qx) {
+    double wx[N];
+#pragma unroll
+    for (int t = 0; t < N; ++t) wx[t] = point_w<ORDER>(qx, t);
+    for (int e = tid; e < 8 * SY * TX; e += TX * TY) {
+      const int c = e / (SY * TX), rem = e - c * SY * TX;
+      const int r = rem / TX, x = rem - r * TX;
+      const double* row = S + (c * SY + r) * SX + x;
+      double smp[N];
+#pragma unroll
+      for (int t = 0; t < N; ++t) smp[t] = row[t];
+      X[e] = wsum<N>(wx, smp);
+    }
+    __syncthreads();
+    if (active && ok) {
+      double st[Q][8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        double smp[N];
+#pragma unroll
+        for (int t = 0; t < N; ++t) smp[t] = X[(c * SY + threadIdx.y + t) * TX + threadIdx.x];
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy) st[qy][c] = point_value<ORDER>(qy, smp);
+      }
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        const St p{st[qy][0], st[qy][1], st[qy][2], st[qy][3],
+                   st[qy][4], st[qy][5], st[qy][6], st[qy][7]};
+        if (!point_admissible(p, gamma)) ok = false;
+        pt[qy][qx] = physical_ez(p);
+      }
+    }
+    __syncthreads();
+  }
+  if (active) {
+    const long long k = g.idx(i, j);
+    double e;
+    if (ok) {
+      double row[Q];
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) row[qy] = gauss_avg<ORDER>(pt[qy]);
+      e = gauss_avg<ORDER>(row);
+    } else {
+      e = physical_ez(load_cell(u, k));
+    }
+    cell_ez[k] = e;
+  }
+  if (!cfl_reduce) return;
+  double local = 0.0;
+  if (i < g.nx && j < g.ny) {
+    const long long k = g.idx(i, j);
+    const double r = (xs[k] + xs[k + 1]) + (ys[k] + ys[k + g.pitch]);
+    local = isfinite(r) ? fmax(0.0, r) : kInf;
+  }
+  local = warp_max(local);
+  if ((tid & 31) == 0) s_max[tid >> 5] = local;
+  __syncthreads();
+  if (tid == 0) {
+    double m = s_max[0];
+    for (int w = 1; w < 8; ++w) m = fmax(m, s_max[w]);
     atomicMax(&ctl->max_rate, dbits(m));
   }
 }
@@ -1160,6 +1426,7 @@ void launch_colloc_check(const Grid& g, const StateP& cand, const StateP* base, 
 template <int DIR, int ORDER>
 static void recon_launch(const StageArgs& a, cudaStream_t s) {
   const Grid& g = a.g;
+
   const dim3 block(kBX, 4);
   const int ni = DIR == 0 ? g.nx + 1 : g.nx + 2 * g.ng;
   const int nj = DIR == 0 ? g.ny + 2 * g.ng : g.ny + 1;
@@ -1178,6 +1445,13 @@ void launch_reconstruct(const StageArgs& a, int dir, cudaStream_t s) {
 template <int DIR, int ORDER>
 static void flux_launch(const StageArgs& a, bool speeds, cudaStream_t s) {
   const Grid& g = a.g;
+  if (ORDER == 5 || ORDER == 7) {
+    const dim3 grid(cdiv(g.nx + 1, 32), g.ny + 1);
+    k_face_flux_q<DIR, ORDER == 5 ? 5 : 7><<<grid, 128, 0, s>>>(
+        g, DIR == 0 ? a.ix : a.iy, DIR == 0 ? a.fx : a.fy, DIR == 0 ? a.xemf : a.yemf,
+        DIR == 0 ? a.xnj : a.ynj, speeds ? (DIR == 0 ? a.xspd : a.yspd) : nullptr, a.gamma, a.ctl);
+    return;
+  }
   const dim3 block(kBX, 4);
   const dim3 grid(cdiv(g.nx + 1, kBX), cdiv(g.ny + 1, 4));
   k_face_flux<DIR, ORDER><<<grid, block, 0, s>>>(
@@ -1193,8 +1467,25 @@ void launch_face_flux(const StageArgs& a, int dir, bool speeds, cudaStream_t s) 
 #undef QB_FLUX
 }
 
+template <int ORDER>
+static void cell_tiled_launch(const StageArgs& a, bool cfl_reduce, cudaStream_t s) {
+  const Grid& g = a.g;
+  constexpr size_t bytes = sizeof(double) * cell_smem_doubles<ORDER>();
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_cell_emf_s<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(bytes));
+    configured = true;
+  }
+  const dim3 grid(cdiv(g.nx + 1, kCellTX), cdiv(g.ny + 1, kCellTY));
+  k_cell_emf_s<ORDER><<<grid, dim3(kCellTX, kCellTY), bytes, s>>>(
+      g, a.u, a.cell_ez, a.xspd, a.yspd, cfl_reduce ? 1 : 0, a.gamma, a.ctl);
+}
+
 void launch_cell_emf(const StageArgs& a, bool cfl_reduce, cudaStream_t s) {
   const Grid& g = a.g;
+  if (a.order == 5) return cell_tiled_launch<5>(a, cfl_reduce, s);
+  if (a.order == 7) return cell_tiled_launch<7>(a, cfl_reduce, s);
   const dim3 block(kBX, 4);
   const dim3 grid(cdiv(g.nx + 1, kBX), cdiv(g.ny + 1, 4));
   const int r = cfl_reduce ? 1 : 0;
