@@ -1,6 +1,7 @@
 /*
- * Measurement extensions of the B200 MHD solver (no counterpart in the
- * reference; used by bench.py).  Same status conventions as quasar_mhd.h.
+ * Extensions of the B200 MHD solver with no counterpart in the reference:
+ * measurement entry points used by bench.py and an allocation-free
+ * diagnostic.  Same status conventions as quasar_mhd.h.
  */
 #ifndef QUASAR_MHD_EXT_H
 #define QUASAR_MHD_EXT_H
@@ -24,6 +25,35 @@ int qmhd_solver_profile_step(qmhd_solver* solver, double* ms_by_phase, int n);
 
 /* Measured FP64 FMA throughput of the current device in TFLOP/s. */
 int qmhd_fp64_fma_peak(double* tflops);
+
+/* Largest nx*ny accepted by qmhd_conserved_cell_totals_device. */
+#define QMHD_TOTALS_DEVICE_MAX_CELLS 67108864LL
+
+/* Mass and energy cell totals of caller-owned device arrays, allocating
+ * nothing.  No counterpart in the reference: it is the compensated sum of
+ * qmhd_solver_conserved_cell_totals (reference mhd_solver.cpp:1376-1382)
+ * applied to the caller's own buffers instead of a solver's state.
+ *
+ * rho, energy: device memory of the calling thread's current device, in the
+ *   solver's padded layout: (nx + 2 nghost) x (ny + 2 nghost) doubles, cell
+ *   (i, j) at (i + nghost) + (nx + 2 nghost)(j + nghost); ghosts are ignored.
+ * stream: a cudaStream_t of that device (NULL = the default stream).  The
+ *   call orders its work after what is already queued on the stream, copies
+ *   the two totals to *mass and *energy_total and synchronizes the stream.
+ *
+ * Scratch is a fixed 256 KiB device array inside the library (one per
+ * device): nothing is allocated on the device, and nothing on the host
+ * unless an error message is formatted.  nx*ny above
+ * QMHD_TOTALS_DEVICE_MAX_CELLS returns QMHD_INVALID_ARGUMENT.  No part of the
+ * scratch has to start at zero: each call writes every slot it reads.
+ * The first call on each device looks up the scratch address (a
+ * cudaGetSymbolAddress); make that first call before any stream capture
+ * begins on the device.  Calls on one device share the one scratch array, so
+ * overlapping calls (other threads, or streams running at once) race and must
+ * be serialised by the caller. */
+int qmhd_conserved_cell_totals_device(const double* rho, const double* energy, int nx, int ny,
+                                      int nghost, void* stream, double* mass,
+                                      double* energy_total);
 
 #ifdef __cplusplus
 }

@@ -23,7 +23,9 @@ EXPORTS = (
     "qmhd_solver_advance", "qmhd_solver_divergence_b_max", "qmhd_solver_conserved_cell_totals",
     "qmhd_solver_last_positivity_substeps", "qmhd_solver_advance_auto",
 )
-EXT_EXPORTS = ("qmhd_solver_time_auto_steps", "qmhd_solver_profile_step", "qmhd_fp64_fma_peak")
+EXT_EXPORTS = ("qmhd_solver_time_auto_steps", "qmhd_solver_profile_step", "qmhd_fp64_fma_peak",
+               "qmhd_conserved_cell_totals_device")
+TOTALS_DEVICE_MAX_CELLS = 67108864
 
 
 class QmhdConfig(ctypes.Structure):
@@ -70,6 +72,8 @@ def lib() -> ctypes.CDLL:
     L.qmhd_solver_time_auto_steps.argtypes = [vp, ctypes.c_int, dp, ip]
     L.qmhd_solver_profile_step.argtypes = [vp, dp, ctypes.c_int]
     L.qmhd_fp64_fma_peak.argtypes = [dp]
+    L.qmhd_conserved_cell_totals_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int, vp, dp, dp]
     _lib = L
     return L
 

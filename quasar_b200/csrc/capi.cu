@@ -2,7 +2,9 @@
 #include "../../include/quasar_mhd.h"
 #include "../../include/quasar_mhd_ext.h"
 #include "mhd_solver.cuh"
+#include "noalloc.cuh"
 
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <stdexcept>
@@ -207,6 +209,79 @@ int qmhd_fp64_fma_peak(double* tflops) {
     *tflops = qb::fp64_fma_peak_tflops();
     if (!(*tflops > 0.0)) throw qb::CudaError("FP64 probe failed");
   });
+}
+
+// Allocation-free totals over caller-owned device arrays: validation, the
+// once-per-device scratch lookup, then the two reductions.  Returns codes
+// directly (no exceptions) so the success path allocates nothing on the host.
+static_assert(QMHD_TOTALS_DEVICE_MAX_CELLS == qb::kTotalsMaxCells, "scratch limit");
+
+int qmhd_conserved_cell_totals_device(const double* rho, const double* energy, int nx, int ny,
+                                      int nghost, void* stream, double* mass,
+                                      double* energy_total) {
+  char msg[256];
+  auto fail = [&](int code) {
+    g_error = msg;
+    return code;
+  };
+  if (!rho || !energy || !mass || !energy_total) {
+    std::snprintf(msg, sizeof msg, "qmhd_conserved_cell_totals_device: null pointer argument");
+    return fail(QMHD_INVALID_ARGUMENT);
+  }
+  if (nx < 1 || ny < 1 || nghost < 0) {
+    std::snprintf(msg, sizeof msg,
+                  "qmhd_conserved_cell_totals_device: need nx >= 1, ny >= 1, nghost >= 0 "
+                  "(got %d, %d, %d)", nx, ny, nghost);
+    return fail(QMHD_INVALID_ARGUMENT);
+  }
+  const long long cells = (long long)nx * ny;
+  if (cells > qb::kTotalsMaxCells) {
+    std::snprintf(msg, sizeof msg,
+                  "qmhd_conserved_cell_totals_device: %lld cells exceed the fixed scratch "
+                  "limit of %lld cells (QMHD_TOTALS_DEVICE_MAX_CELLS)",
+                  cells, (long long)qb::kTotalsMaxCells);
+    return fail(QMHD_INVALID_ARGUMENT);
+  }
+  int device = -1;
+  cudaError_t rc = cudaGetDevice(&device);
+  if (rc != cudaSuccess) {
+    std::snprintf(msg, sizeof msg, "qmhd_conserved_cell_totals_device: cudaGetDevice: %s",
+                  cudaGetErrorString(rc));
+    return fail(QMHD_DEVICE_ERROR);
+  }
+  for (const double* p : {rho, energy}) {
+    cudaPointerAttributes a{};
+    rc = cudaPointerGetAttributes(&a, p);
+    if (rc != cudaSuccess ||
+        !(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) ||
+        a.device != device) {
+      cudaGetLastError();
+      std::snprintf(msg, sizeof msg,
+                    "qmhd_conserved_cell_totals_device: %s is not device memory of the "
+                    "current device %d", p == rho ? "rho" : "energy", device);
+      return fail(QMHD_INVALID_ARGUMENT);
+    }
+  }
+  double* scratch = nullptr;
+  rc = qb::totals_scratch(device, &scratch);
+  if (rc != cudaSuccess) {
+    std::snprintf(msg, sizeof msg,
+                  "qmhd_conserved_cell_totals_device: scratch lookup on device %d: %s", device,
+                  cudaGetErrorString(rc));
+    return fail(QMHD_DEVICE_ERROR);
+  }
+  double totals[2];
+  rc = qb::launch_totals_noalloc(rho, energy, nx, ny, nghost, scratch, (cudaStream_t)stream,
+                                 totals);
+  if (rc != cudaSuccess) {
+    std::snprintf(msg, sizeof msg, "qmhd_conserved_cell_totals_device: %s",
+                  cudaGetErrorString(rc));
+    return fail(QMHD_DEVICE_ERROR);
+  }
+  *mass = totals[0];
+  *energy_total = totals[1];
+  g_error.clear();
+  return QMHD_OK;
 }
 
 }  // extern "C"
