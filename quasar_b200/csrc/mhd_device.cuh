@@ -149,15 +149,15 @@ __device__ __forceinline__ double pressure_f(const St& u, double gamma, double i
   const double m = 0.5 * (u.bx * u.bx + u.by * u.by + u.bz * u.bz);
   return (gamma - 1.0) * ((u.E - k) - m);
 }
-// fast magnetosonic speed normal to x from p and 1/rho (mhd_state.hpp:148-182)
+// fast magnetosonic speed normal to x from p and 1/rho (mhd_state.hpp:148-182);
+// discriminant as (a^2 - b^2)^2 + 4 a^2 b_t^2, free of cancellation
 __device__ __forceinline__ double fast_x_f(const St& u, double p, double ir, double gamma) {
   const double a2 = p > 0.0 ? gamma * p * ir : 0.0;
   const double bn2 = u.bx * u.bx * ir;
-  const double b2 = (u.bx * u.bx + u.by * u.by + u.bz * u.bz) * ir;
-  const double sum = a2 + b2;
-  double disc = sum * sum - 4.0 * a2 * bn2;
-  if (disc < 0.0) disc = 0.0;
-  return sqrt(0.5 * (sum + sqrt(disc)));
+  const double bt2 = (u.by * u.by + u.bz * u.bz) * ir;
+  const double d = a2 - (bn2 + bt2);
+  const double disc = d * d + 4.0 * a2 * bt2;
+  return sqrt(0.5 * ((a2 + bn2 + bt2) + sqrt(disc)));
 }
 
 __device__ __forceinline__ Pr to_prim(const St& u, double gamma) {
@@ -290,12 +290,12 @@ __device__ __forceinline__ double mp_recon(const double* v, bool& fired) {
     if (W == 5) {
       const double sum = 2.0 * (v[0] * is) - 13.0 * (v[1] * is) + 47.0 * (v[2] * is) +
                          27.0 * (v[3] * is) - 3.0 * (v[4] * is);
-      vl = (sum / 60.0) * s;
+      vl = (sum * (1.0 / 60.0)) * s;
     } else {
       const double sum = -3.0 * (v[0] * is) + 25.0 * (v[1] * is) - 101.0 * (v[2] * is) +
                          319.0 * (v[3] * is) + 214.0 * (v[4] * is) - 38.0 * (v[5] * is) +
                          4.0 * (v[6] * is);
-      vl = (sum / 420.0) * s;
+      vl = (sum * (1.0 / 420.0)) * s;
     }
   }
   constexpr int o = W == 5 ? 0 : 1;

@@ -327,8 +327,9 @@ __device__ __forceinline__ void set_normal_b(St& s, double v) {
 // (mhd_eigensystem.hpp:63-171), shared by all seven waves.
 struct Eg {
   double rho, sr, cf, cs, a, af, as, b1, b2, sbn, vn, vt1, vt2, bt1, bt2;
-  double ia2, ra2, gm1, hv2, ir;
+  double ia2, ra2, gm1, hv2, ir, isr, igm;
 };
+constexpr double kRs2 = 0.7071067811865475;  // 1/sqrt(2) rounded
 
 __device__ __forceinline__ Eg eig_scalars(const St& s, double gamma) {
   Eg e;
@@ -345,8 +346,8 @@ __device__ __forceinline__ Eg eig_scalars(const St& s, double gamma) {
     const double cfn = e.cf / sc, csn = e.cs / sc, an = e.a / sc;
     const double den = sub(mul(cfn, cfn), mul(csn, csn));
     if (den <= mul(64.0 * kEps, add(mul(cfn, cfn), mul(csn, csn)))) {
-      e.af = 1.0 / sqrt(2.0);
-      e.as = 1.0 / sqrt(2.0);
+      e.af = kRs2;
+      e.as = kRs2;
     } else {
       const double af2 = sub(mul(an, an), mul(csn, csn)) / den;
       const double as2 = sub(mul(cfn, cfn), mul(an, an)) / den;
@@ -358,8 +359,8 @@ __device__ __forceinline__ Eg eig_scalars(const St& s, double gamma) {
     const double bt = scaled_norm3(w.by, w.bz, 0.0);
     const double fs = e.a > ca ? e.a : ca;
     if (bt == 0.0 || bt / e.sr <= 64.0 * kEps * (fs + kTiny)) {
-      e.b1 = 1.0 / sqrt(2.0);
-      e.b2 = 1.0 / sqrt(2.0);
+      e.b1 = kRs2;
+      e.b2 = kRs2;
     } else {
       e.b1 = w.by / bt;
       e.b2 = w.bz / bt;
@@ -374,6 +375,8 @@ __device__ __forceinline__ Eg eig_scalars(const St& s, double gamma) {
   e.gm1 = gamma - 1.0;
   e.hv2 = half_sq3(e.vn, e.vt1, e.vt2);
   e.ir = 1.0 / e.rho;
+  e.isr = 1.0 / e.sr;
+  e.igm = 1.0 / e.gm1;
   return e;
 }
 
@@ -388,7 +391,7 @@ __device__ __forceinline__ void wave_vectors(const Eg& e, int k, double* lp, dou
   const double rho = e.rho;
   const double qf = e.cf * e.af * e.sbn, qs = e.cs * e.as * e.sbn;
   const double Af = e.a * e.af * e.sr, As = e.a * e.as * e.sr;
-  const double Nf = 0.5 * e.ia2, s2 = 1.0 / sqrt(2.0);
+  const double Nf = 0.5 * e.ia2, s2 = kRs2;
   if (k == 0 || k == 6) {
     rp[0] = rho * e.af;
     rp[1] = k == 0 ? -e.af * e.cf : e.af * e.cf;
@@ -400,9 +403,9 @@ __device__ __forceinline__ void wave_vectors(const Eg& e, int k, double* lp, dou
     lp[1] = k == 0 ? -Nf * e.af * e.cf : Nf * e.af * e.cf;
     lp[2] = k == 0 ? Nf * qs * e.b1 : -Nf * qs * e.b1;
     lp[3] = k == 0 ? Nf * qs * e.b2 : -Nf * qs * e.b2;
-    lp[4] = Nf * e.af / rho;
-    lp[5] = Nf * As * e.b1 / rho;
-    lp[6] = Nf * As * e.b2 / rho;
+    lp[4] = Nf * e.af * e.ir;
+    lp[5] = Nf * As * e.b1 * e.ir;
+    lp[6] = Nf * As * e.b2 * e.ir;
   } else if (k == 1 || k == 5) {
     rp[2] = -e.b2 * s2;
     rp[3] = e.b1 * s2;
@@ -410,8 +413,8 @@ __device__ __forceinline__ void wave_vectors(const Eg& e, int k, double* lp, dou
     rp[6] = k == 1 ? e.sbn * e.b1 * s2 * e.sr : -e.sbn * e.b1 * s2 * e.sr;
     lp[2] = -e.b2 * s2;
     lp[3] = e.b1 * s2;
-    lp[5] = k == 1 ? -e.sbn * e.b2 * s2 / e.sr : e.sbn * e.b2 * s2 / e.sr;
-    lp[6] = k == 1 ? e.sbn * e.b1 * s2 / e.sr : -e.sbn * e.b1 * s2 / e.sr;
+    lp[5] = k == 1 ? -e.sbn * e.b2 * s2 * e.isr : e.sbn * e.b2 * s2 * e.isr;
+    lp[6] = k == 1 ? e.sbn * e.b1 * s2 * e.isr : -e.sbn * e.b1 * s2 * e.isr;
   } else if (k == 2 || k == 4) {
     rp[0] = rho * e.as;
     rp[1] = k == 2 ? -e.as * e.cs : e.as * e.cs;
@@ -423,9 +426,9 @@ __device__ __forceinline__ void wave_vectors(const Eg& e, int k, double* lp, dou
     lp[1] = k == 2 ? -Nf * e.as * e.cs : Nf * e.as * e.cs;
     lp[2] = k == 2 ? -Nf * qf * e.b1 : Nf * qf * e.b1;
     lp[3] = k == 2 ? -Nf * qf * e.b2 : Nf * qf * e.b2;
-    lp[4] = Nf * e.as / rho;
-    lp[5] = -Nf * Af * e.b1 / rho;
-    lp[6] = -Nf * Af * e.b2 / rho;
+    lp[4] = Nf * e.as * e.ir;
+    lp[5] = -Nf * Af * e.b1 * e.ir;
+    lp[6] = -Nf * Af * e.b2 * e.ir;
   } else if (k == 3) {
     rp[0] = 1.0;
     lp[0] = 1.0;
@@ -453,9 +456,18 @@ __device__ __forceinline__ void conserved_row_col(const Eg& e, int k, double* Lr
   Rc[2] = e.vt1 * rp[0] + e.rho * rp[2];
   Rc[3] = e.vt2 * rp[0] + e.rho * rp[3];
   Rc[4] = (((((e.hv2 * rp[0] + (e.rho * e.vn) * rp[1]) + (e.rho * e.vt1) * rp[2]) +
-             (e.rho * e.vt2) * rp[3]) + (1.0 / gv) * rp[4]) + e.bt1 * rp[5]) + e.bt2 * rp[6];
+             (e.rho * e.vt2) * rp[3]) + e.igm * rp[4]) + e.bt1 * rp[5]) + e.bt2 * rp[6];
   Rc[5] = rp[5];
   Rc[6] = rp[6];
+}
+
+__device__ __forceinline__ void conserved_row(const Eg& e, int k, double* Lr) {
+  double Rc[7];
+  conserved_row_col(e, k, Lr, Rc);
+}
+__device__ __forceinline__ void conserved_col(const Eg& e, int k, double* Rc) {
+  double Lr[7];
+  conserved_row_col(e, k, Lr, Rc);
 }
 
 template <int DIR, int H>
@@ -474,26 +486,28 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
   ref.bz = 0.5 * cl.bz + 0.5 * cr.bz;
   const St c = rot<DIR>(ref);
   const Eg e = eig_scalars(c, gamma);
-  // L R = I check (mhd_eigensystem.hpp:416-430): all R columns resident,
-  // L rows one at a time
+  // L R = I check (mhd_eigensystem.hpp:416-430), R columns resident in two
+  // halves (4 + 3) against L rows rebuilt one at a time
   bool usable = true;
-  {
-    double R[7][7];
 #pragma unroll
-    for (int j = 0; j < 7; ++j) {
-      double Lr[7];
-      conserved_row_col(e, j, Lr, R[j]);
-    }
+  for (int half = 0; half < 2; ++half) {
+    constexpr int kCols = 4;
+    const int j0 = half * kCols, nj = half == 0 ? kCols : 7 - kCols;
+    double R[kCols][7];
+#pragma unroll
+    for (int jj = 0; jj < kCols; ++jj)
+      if (jj < nj) conserved_col(e, j0 + jj, R[jj]);
 #pragma unroll 1
     for (int i = 0; i < 7; ++i) {
-      double Lr[7], Rc[7];
-      conserved_row_col(e, i, Lr, Rc);
+      double Lr[7];
+      conserved_row(e, i, Lr);
 #pragma unroll
-      for (int j = 0; j < 7; ++j) {
+      for (int jj = 0; jj < kCols; ++jj) {
+        if (jj >= nj) continue;
         double dot = 0.0;
 #pragma unroll
-        for (int m = 0; m < 7; ++m) dot += Lr[m] * R[j][m];
-        const double expect = i == j ? 1.0 : 0.0;
+        for (int m = 0; m < 7; ++m) dot += Lr[m] * R[jj][m];
+        const double expect = i == j0 + jj ? 1.0 : 0.0;
         if (!isfinite(dot) || fabs(dot - expect) > 1024.0 * kEps) usable = false;
       }
     }
@@ -519,15 +533,12 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
   }
 #pragma unroll 1
   for (int k = 0; k < 7; ++k) {
-    double Lr[7], Rc[7];
+    double Lr[7];
     if (usable) {
-      conserved_row_col(e, k, Lr, Rc);
+      conserved_row(e, k, Lr);
     } else {
 #pragma unroll
-      for (int v = 0; v < 7; ++v) {
-        Lr[v] = v == k ? 1.0 : 0.0;
-        Rc[v] = v == k ? 1.0 : 0.0;
-      }
+      for (int v = 0; v < 7; ++v) Lr[v] = v == k ? 1.0 : 0.0;
     }
     double ch[S];
 #pragma unroll
@@ -545,6 +556,13 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
 #pragma unroll
     for (int s = 0; s < W; ++s) win[s] = ch[W - s];
     const double wr = mp_recon<W>(win, f);
+    double Rc[7];
+    if (usable) {
+      conserved_col(e, k, Rc);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 7; ++v) Rc[v] = v == k ? 1.0 : 0.0;
+    }
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
       dl[v] += Rc[v] * wl;
@@ -659,33 +677,28 @@ struct Spd {
   double v, f;
 };
 
-// One side's |v_n| and fast speed (mhd_reduce.hip:254-325).  Kept in the
-// reference's scaled form: dt is the max of these and, at a degenerate fan
-// (a^2 == b_n^2, b_t == 0), the discriminant's rounding is amplified to
-// sqrt(eps), so any reassociation moves dt by ~1e-9.
+// One side's |v_n| and fast speed (mhd_reduce.hip:254-325), with one
+// reciprocal of rho.  The discriminant is formed as (a^2 - b^2)^2 + 4 a^2 b_t^2,
+// which equals the reference's (a^2 + b^2)^2 - 4 a^2 b_n^2 but has no
+// cancellation: where the reference's rounding is amplified to sqrt(eps) (a
+// degenerate fan, a == b_n with b_t == 0) this form stays accurate to a few
+// ulps, and elsewhere both agree to rounding.
 template <int DIR>
 __device__ Spd speed_parts(const St& s, double gamma) {
-  const double p = pressure(s, gamma);
   if (!(isfinite(s.rho) && s.rho > 0.0 && isfinite(s.mx) && isfinite(s.my) &&
-        isfinite(s.mz) && isfinite(s.E) && isfinite(s.bx) && isfinite(s.by) &&
-        isfinite(s.bz) && isfinite(p) && p > 0.0))
+        isfinite(s.mz) && isfinite(s.E) && isfinite(s.bx) && isfinite(s.by) && isfinite(s.bz)))
     return Spd{kInf, kInf};
-  const double sr = sqrt(s.rho);
-  const double sound = mul(sqrt(gamma), sqrt(p)) / sr;
-  const double ax = s.bx / sr, ay = s.by / sr, az = s.bz / sr;
-  if (!(isfinite(sound) && isfinite(ax) && isfinite(ay) && isfinite(az))) return Spd{kInf, kInf};
-  const double ca = scaled_norm3(ax, ay, az);
-  const double can = fabs(DIR == 0 ? ax : ay);
-  const double scale = fmax(sound, ca);
-  double fast = 0.0;
-  if (scale > 0.0) {
-    const double an = sound / scale, bn = ca / scale, cn = can / scale;
-    const double a2 = mul(an, an), b2 = mul(bn, bn), sum = add(a2, b2);
-    double disc = sub(mul(sum, sum), mul(mul(mul(4.0, a2), cn), cn));
-    if (disc < 0.0) disc = 0.0;
-    fast = mul(scale, sqrt(mul(0.5, add(sum, sqrt(disc)))));
-  }
-  const double vel = fabs(DIR == 0 ? s.mx : s.my) / s.rho;
+  const double ir = 1.0 / s.rho;
+  const double p = pressure_f(s, gamma, ir);
+  if (!(isfinite(p) && p > 0.0)) return Spd{kInf, kInf};
+  const double bn = DIR == 0 ? s.bx : s.by, b1 = DIR == 0 ? s.by : s.bx;
+  const double a2 = gamma * p * ir;
+  const double bn2 = bn * bn * ir;
+  const double bt2 = (b1 * b1 + s.bz * s.bz) * ir;
+  const double d = a2 - (bn2 + bt2);
+  const double disc = d * d + 4.0 * a2 * bt2;
+  const double fast = sqrt(0.5 * ((a2 + bn2 + bt2) + sqrt(disc)));
+  const double vel = fabs(DIR == 0 ? s.mx : s.my) * ir;
   if (!(isfinite(vel) && isfinite(fast))) return Spd{kInf, kInf};
   return Spd{vel, fast};
 }
@@ -700,9 +713,11 @@ __device__ __forceinline__ double face_rate(const St& l, const St& r, double gam
 }
 
 __device__ __forceinline__ St iface(const IfaceP& v, long long k, bool left) {
-  double* const* a = left ? v.L : v.R;
-  return St{__ldg(a[0] + k), __ldg(a[1] + k), __ldg(a[2] + k), __ldg(a[3] + k),
-            __ldg(a[4] + k), __ldg(a[5] + k), __ldg(a[6] + k), __ldg(a[7] + k)};
+  if (left)
+    return St{__ldg(v.L[0] + k), __ldg(v.L[1] + k), __ldg(v.L[2] + k), __ldg(v.L[3] + k),
+              __ldg(v.L[4] + k), __ldg(v.L[5] + k), __ldg(v.L[6] + k), __ldg(v.L[7] + k)};
+  return St{__ldg(v.R[0] + k), __ldg(v.R[1] + k), __ldg(v.R[2] + k), __ldg(v.R[3] + k),
+            __ldg(v.R[4] + k), __ldg(v.R[5] + k), __ldg(v.R[6] + k), __ldg(v.R[7] + k)};
 }
 
 template <int DIR, int ORDER>
@@ -831,7 +846,7 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
 namespace {
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128) k_face_flux_q(Grid g, IfaceP in, FluxP out, double* emf,
+__global__ void __launch_bounds__(128, 4) k_face_flux_q(Grid g, IfaceP in, FluxP out, double* emf,
                                                      int* nj, double* spd, double gamma,
                                                      const Ctl* ctl) {
   constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
@@ -906,8 +921,10 @@ __global__ void __launch_bounds__(128) k_face_flux_q(Grid g, IfaceP in, FluxP ou
   // stores split over the group: lane q writes components q and q+4
   const double lo = lane == 0 ? res[0] : lane == 1 ? res[1] : lane == 2 ? res[2] : res[3];
   const double hi = lane == 0 ? res[4] : lane == 1 ? res[5] : lane == 2 ? res[6] : res[7];
-  out.f[lane][k] = lo;
-  out.f[lane + 4][k] = hi;
+  double* const flo = lane == 0 ? out.f[0] : lane == 1 ? out.f[1] : lane == 2 ? out.f[2] : out.f[3];
+  double* const fhi = lane == 0 ? out.f[4] : lane == 1 ? out.f[5] : lane == 2 ? out.f[6] : out.f[7];
+  flo[k] = lo;
+  fhi[k] = hi;
   if (lane == 0) emf[k] = DIR == 0 ? -res[6] : res[5];
   if (spd) {
     rate = fmax(rate, __shfl_xor_sync(gmask, rate, 1, 4));
@@ -1222,6 +1239,83 @@ __global__ void __launch_bounds__(128) k_corner_emf(Grid g, const double* cell_e
   ez[k] = v;
 }
 
+// Same corner EMF with the block's cell E_z stencil staged in shared memory:
+// a (32 + NT - 1) x (4 + NT - 1) tile of the mapped cell table, so each
+// corner's NT x NT reads are shared-memory loads.  Tile coordinates go
+// through face_index like every CT table read, which keeps them inside the
+// padded grid for any block position.
+template <int ORDER>
+__global__ void __launch_bounds__(128, 4) k_corner_emf_s(Grid g, const double* cell_ez,
+                                                      const double* xemf, const double* yemf,
+                                                      const int* xnj, const int* ynj, double* ez,
+                                                      const Ctl* ctl) {
+  constexpr int LO = ORDER >= 7 ? -4 : ORDER >= 5 ? -3 : -1;
+  constexpr int NT = ORDER >= 7 ? 8 : ORDER >= 5 ? 6 : 2;
+  constexpr int TW = 32 + NT - 1, TH = 4 + NT - 1;
+  __shared__ double tile[TH][TW];
+  if (ctl->status) return;  // uniform over the block
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 4;
+  for (int t = tid; t < TH * TW; t += 128) {
+    const int a = t % TW, b = t / TW;
+    const int mi = face_index(i0 + LO + a, g.nx, g.bc[0], g.bc[1]);
+    const int mj = face_index(j0 + LO + b, g.ny, g.bc[2], g.bc[3]);
+    tile[b][a] = __ldg(cell_ez + g.idx(mi, mj));
+  }
+  __syncthreads();
+  const int i = i0 + tx, j = j0 + ty;
+  if (i > g.nx || j > g.ny) return;
+  const long long k = g.idx(i, j);
+  const bool conducting = (i == 0 && g.bc[0] == 2) || (i == g.nx && g.bc[1] == 2) ||
+                          (j == 0 && g.bc[2] == 2) || (j == g.ny && g.bc[3] == 2);
+  if (conducting) {
+    ez[k] = 0.0;
+    return;
+  }
+  const int fi = face_index(i, g.nx, g.bc[0], g.bc[1]);
+  const int fj = face_index(j, g.ny, g.bc[2], g.bc[3]);
+  double e[NT], line[NT];
+  bool nj_y = true, nj_x = true;
+#pragma unroll
+  for (int q = 0; q < NT; ++q) {
+    const int mj = face_index(j + LO + q, g.ny, g.bc[2], g.bc[3]);
+    const long long kx = g.idx(fi, mj);
+    e[q] = __ldg(xemf + kx);
+    nj_x = nj_x && __ldg(xnj + kx) != 0;
+  }
+  const double ex = edge_interp<NT>(e);
+#pragma unroll
+  for (int q = 0; q < NT; ++q) {
+    const int mi = face_index(i + LO + q, g.nx, g.bc[0], g.bc[1]);
+    const long long ky = g.idx(mi, fj);
+    e[q] = __ldg(yemf + ky);
+    nj_y = nj_y && __ldg(ynj + ky) != 0;
+  }
+  const double ey = edge_interp<NT>(e);
+  bool const_x = true, const_y = true;
+#pragma unroll
+  for (int q = 0; q < NT; ++q) {
+    double c[NT];
+#pragma unroll
+    for (int p = 0; p < NT; ++p) c[p] = tile[ty + q][tx + p];
+#pragma unroll
+    for (int p = 1; p < NT; ++p) const_x = const_x && (c[p] == c[0]);
+    if (q > 0) {
+#pragma unroll
+      for (int p = 0; p < NT; ++p) const_y = const_y && (c[p] == tile[ty][tx + p]);
+    }
+    line[q] = edge_interp<NT>(c);
+  }
+  const double centred = edge_interp<NT>(line);
+  const bool x_only = nj_y && const_y;
+  const bool y_only = nj_x && const_x;
+  double v;
+  if (x_only && !y_only) v = ex;
+  else if (y_only && !x_only) v = ey;
+  else v = crsum3(ex, ey, -centred);
+  ez[k] = v;
+}
+
 // Flux difference + EMF curl + Shu-Osher combine (mhd_update.hip:21-206,
 // mhd_ct.hip:893-931, mhd_solver.cpp:840-874).  Writes cells and the owned
 // high faces of the output; ghosts are closed by fill_ghosts afterwards.
@@ -1504,8 +1598,8 @@ void launch_corner_emf(const StageArgs& a, cudaStream_t s) {
   switch (a.order) {
     case 1:
     case 2: k_corner_emf<2><<<grid, block, 0, s>>>(g, a.cell_ez, a.xemf, a.yemf, a.xnj, a.ynj, a.ez, a.ctl); break;
-    case 5: k_corner_emf<5><<<grid, block, 0, s>>>(g, a.cell_ez, a.xemf, a.yemf, a.xnj, a.ynj, a.ez, a.ctl); break;
-    default: k_corner_emf<7><<<grid, block, 0, s>>>(g, a.cell_ez, a.xemf, a.yemf, a.xnj, a.ynj, a.ez, a.ctl);
+    case 5: k_corner_emf_s<5><<<grid, block, 0, s>>>(g, a.cell_ez, a.xemf, a.yemf, a.xnj, a.ynj, a.ez, a.ctl); break;
+    default: k_corner_emf_s<7><<<grid, block, 0, s>>>(g, a.cell_ez, a.xemf, a.yemf, a.xnj, a.ynj, a.ez, a.ctl);
   }
 }
 
