@@ -26,6 +26,9 @@ EXPORTS = (
 EXT_EXPORTS = ("qmhd_solver_time_auto_steps", "qmhd_solver_profile_step", "qmhd_fp64_fma_peak",
                "qmhd_conserved_cell_totals_device")
 TOTALS_DEVICE_MAX_CELLS = 67108864
+BATCH_EXPORTS = ("qmhd_batch_create", "qmhd_batch_destroy", "qmhd_batch_size", "qmhd_batch_zones",
+                 "qmhd_batch_instance", "qmhd_batch_advance", "qmhd_batch_time_steps",
+                 "qmhd_batch_autotune", "qmhd_batch_set_tuning")
 
 
 class QmhdConfig(ctypes.Structure):
@@ -74,6 +77,18 @@ def lib() -> ctypes.CDLL:
     L.qmhd_fp64_fma_peak.argtypes = [dp]
     L.qmhd_conserved_cell_totals_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int,
                                                     ctypes.c_int, vp, dp, dp]
+    L.qmhd_batch_create.argtypes = [ctypes.POINTER(QmhdConfig), ctypes.c_int, ctypes.POINTER(vp)]
+    L.qmhd_batch_destroy.argtypes = [vp]
+    L.qmhd_batch_destroy.restype = None
+    L.qmhd_batch_size.argtypes = [vp]
+    L.qmhd_batch_zones.argtypes = [vp]
+    L.qmhd_batch_zones.restype = ctypes.c_longlong
+    L.qmhd_batch_instance.argtypes = [vp, ctypes.c_int]
+    L.qmhd_batch_instance.restype = vp
+    L.qmhd_batch_advance.argtypes = [vp, ctypes.c_int, ip]
+    L.qmhd_batch_time_steps.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(ctypes.c_longlong)]
+    L.qmhd_batch_autotune.argtypes = [vp, ip, ip]
+    L.qmhd_batch_set_tuning.argtypes = [vp, ip]
     _lib = L
     return L
 

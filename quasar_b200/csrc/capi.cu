@@ -1,22 +1,33 @@
 // extern "C" boundary over qb::MhdSolver2D (declarations: include/quasar_mhd.h).
 #include "../../include/quasar_mhd.h"
 #include "../../include/quasar_mhd_ext.h"
+#include "../../include/quasar_mhd_batch.h"
+#include "mhd_batch.cuh"
 #include "mhd_solver.cuh"
 #include "noalloc.cuh"
 
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <memory>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace qb {
 double fp64_fma_peak_tflops();
 }
 
+// A solver handle: an owned solver, or a view of one instance of a batch
+// (owned by the batch; destroying a view does nothing).
 struct qmhd_solver {
-  qb::MhdSolver2D impl;
-  explicit qmhd_solver(const qb::Config& c) : impl(c) {}
+  qb::MhdSolver2D* impl = nullptr;
+  bool owned = false;
+};
+
+struct qmhd_batch {
+  std::unique_ptr<qb::MhdBatch2D> impl;
+  std::vector<qmhd_solver> views;
 };
 
 namespace {
@@ -66,6 +77,21 @@ void need(const void* p) {
   if (!p) throw std::invalid_argument("qmhd: null pointer argument");
 }
 
+qb::Config to_config(const qmhd_config& q) {
+  qb::Config c;
+  c.nx = q.nx;
+  c.ny = q.ny;
+  c.lx = q.lx;
+  c.ly = q.ly;
+  c.ox = q.origin_x;
+  c.oy = q.origin_y;
+  c.order = q.reconstruction_order;
+  c.gamma = q.gamma;
+  c.cfl = q.cfl;
+  for (int s = 0; s < 4; ++s) c.bc[s] = q.boundary[s];
+  return c;
+}
+
 }  // namespace
 
 extern "C" {
@@ -77,27 +103,21 @@ int qmhd_solver_create(const qmhd_config* config, qmhd_solver** out) {
     need(config);
     need(out);
     *out = nullptr;
-    qb::Config c;
-    c.nx = config->nx;
-    c.ny = config->ny;
-    c.lx = config->lx;
-    c.ly = config->ly;
-    c.ox = config->origin_x;
-    c.oy = config->origin_y;
-    c.order = config->reconstruction_order;
-    c.gamma = config->gamma;
-    c.cfl = config->cfl;
-    for (int s = 0; s < 4; ++s) c.bc[s] = config->boundary[s];
-    *out = new qmhd_solver(c);
+    std::unique_ptr<qb::MhdSolver2D> impl(new qb::MhdSolver2D(to_config(*config)));
+    *out = new qmhd_solver{impl.release(), true};
   });
 }
 
-void qmhd_solver_destroy(qmhd_solver* solver) { delete solver; }
+void qmhd_solver_destroy(qmhd_solver* solver) {
+  if (!solver || !solver->owned) return;
+  delete solver->impl;
+  delete solver;
+}
 
 int qmhd_solver_grid(const qmhd_solver* s, int* nx, int* ny, int* nghost) {
   return guarded([&] {
     need(s);
-    const qb::Grid& g = s->impl.grid();
+    const qb::Grid& g = s->impl->grid();
     if (nx) *nx = g.nx;
     if (ny) *ny = g.ny;
     if (nghost) *nghost = g.ng;
@@ -105,7 +125,7 @@ int qmhd_solver_grid(const qmhd_solver* s, int* nx, int* ny, int* nghost) {
 }
 
 long long qmhd_solver_storage_size(const qmhd_solver* s) {
-  return s ? s->impl.storage_size() : -1;
+  return s ? s->impl->storage_size() : -1;
 }
 
 int qmhd_solver_seed_state(qmhd_solver* s, const char* component, const double* values,
@@ -113,7 +133,7 @@ int qmhd_solver_seed_state(qmhd_solver* s, const char* component, const double* 
   return guarded([&] {
     need(s);
     need(values);
-    s->impl.seed_state(component_index(component, false), values, (long long)n);
+    s->impl->seed_state(component_index(component, false), values, (long long)n);
   });
 }
 
@@ -122,7 +142,7 @@ int qmhd_solver_state_component_to_host(qmhd_solver* s, const char* component, d
   return guarded([&] {
     need(s);
     need(out);
-    s->impl.state_component_to_host(component_index(component, true), out, (long long)n);
+    s->impl->state_component_to_host(component_index(component, true), out, (long long)n);
   });
 }
 
@@ -130,28 +150,28 @@ int qmhd_solver_cfl_limit(qmhd_solver* s, double* dt) {
   return guarded([&] {
     need(s);
     need(dt);
-    *dt = s->impl.cfl_limit();
+    *dt = s->impl->cfl_limit();
   });
 }
 
 int qmhd_solver_step(qmhd_solver* s, double dt) {
   return guarded([&] {
     need(s);
-    s->impl.step(dt);
+    s->impl->step(dt);
   });
 }
 
 int qmhd_solver_step_unchecked(qmhd_solver* s, double dt) {
   return guarded([&] {
     need(s);
-    s->impl.step_unchecked(dt);
+    s->impl->step_unchecked(dt);
   });
 }
 
 int qmhd_solver_advance(qmhd_solver* s, double t_end, double dt) {
   return guarded([&] {
     need(s);
-    s->impl.advance(t_end, dt);
+    s->impl->advance(t_end, dt);
   });
 }
 
@@ -159,7 +179,7 @@ int qmhd_solver_divergence_b_max(qmhd_solver* s, double* out) {
   return guarded([&] {
     need(s);
     need(out);
-    *out = s->impl.divergence_b_max();
+    *out = s->impl->divergence_b_max();
   });
 }
 
@@ -168,12 +188,12 @@ int qmhd_solver_conserved_cell_totals(qmhd_solver* s, double* mass, double* ener
     need(s);
     need(mass);
     need(energy);
-    s->impl.conserved_cell_totals(mass, energy);
+    s->impl->conserved_cell_totals(mass, energy);
   });
 }
 
 int qmhd_solver_last_positivity_substeps(const qmhd_solver* s) {
-  return s ? s->impl.last_positivity_substeps() : -1;
+  return s ? s->impl->last_positivity_substeps() : -1;
 }
 
 int qmhd_solver_advance_auto(qmhd_solver* s, double* t, double t_end, int max_steps,
@@ -181,7 +201,7 @@ int qmhd_solver_advance_auto(qmhd_solver* s, double* t, double t_end, int max_st
   return guarded([&] {
     need(s);
     need(t);
-    const int n = s->impl.advance_auto(t, t_end, max_steps);
+    const int n = s->impl->advance_auto(t, t_end, max_steps);
     if (steps_taken) *steps_taken = n;
   });
 }
@@ -190,7 +210,7 @@ int qmhd_solver_time_auto_steps(qmhd_solver* s, int steps, double* ms, int* done
   return guarded([&] {
     need(s);
     need(ms);
-    *ms = s->impl.time_auto_steps(steps, done);
+    *ms = s->impl->time_auto_steps(steps, done);
   });
 }
 
@@ -199,7 +219,7 @@ int qmhd_solver_profile_step(qmhd_solver* s, double* ms, int n) {
     need(s);
     need(ms);
     if (n < qb::MhdSolver2D::kPhases) throw std::invalid_argument("qmhd: phase buffer too small");
-    s->impl.profile_step(ms);
+    s->impl->profile_step(ms);
   });
 }
 
@@ -210,6 +230,71 @@ int qmhd_fp64_fma_peak(double* tflops) {
     if (!(*tflops > 0.0)) throw qb::CudaError("FP64 probe failed");
   });
 }
+
+// ---- batched instances (include/quasar_mhd_batch.h) ------------------------
+int qmhd_batch_create(const qmhd_config* configs, int n, qmhd_batch** out) {
+  return guarded([&] {
+    need(configs);
+    need(out);
+    *out = nullptr;
+    if (n < 1) throw std::invalid_argument("qmhd_batch_create: need at least one instance");
+    std::vector<qb::Config> cfgs;
+    for (int i = 0; i < n; ++i) cfgs.push_back(to_config(configs[i]));
+    std::unique_ptr<qmhd_batch> b(new qmhd_batch);
+    b->impl.reset(new qb::MhdBatch2D(cfgs));
+    b->views.resize(size_t(n));
+    for (int i = 0; i < n; ++i) b->views[size_t(i)] = qmhd_solver{&b->impl->instance(i), false};
+    *out = b.release();
+  });
+}
+
+void qmhd_batch_destroy(qmhd_batch* batch) { delete batch; }
+
+int qmhd_batch_size(const qmhd_batch* batch) { return batch ? int(batch->views.size()) : -1; }
+
+qmhd_solver* qmhd_batch_instance(qmhd_batch* batch, int i) {
+  if (!batch || i < 0 || i >= int(batch->views.size())) return nullptr;
+  return &batch->views[size_t(i)];
+}
+
+int qmhd_batch_advance(qmhd_batch* batch, int steps, int* steps_taken) {
+  return guarded([&] {
+    need(batch);
+    if (steps < 0) throw std::invalid_argument("qmhd_batch_advance: steps must be >= 0");
+    batch->impl->advance(steps, steps_taken);
+  });
+}
+
+int qmhd_batch_time_steps(qmhd_batch* batch, int steps, double* ms, long long* zone_updates) {
+  return guarded([&] {
+    need(batch);
+    need(ms);
+    if (steps < 1) throw std::invalid_argument("qmhd_batch_time_steps: steps must be >= 1");
+    *ms = batch->impl->time_steps(steps, zone_updates);
+  });
+}
+
+int qmhd_batch_autotune(qmhd_batch* batch, int* ctas_per_sm, int* trial_steps) {
+  return guarded([&] {
+    need(batch);
+    const int t = batch->impl->autotune();
+    if (trial_steps) *trial_steps = t;
+    if (ctas_per_sm)
+      for (int ph = 0; ph < QMHD_BATCH_PHASES; ++ph) ctas_per_sm[ph] = batch->impl->tuning()[size_t(ph)];
+  });
+}
+
+int qmhd_batch_set_tuning(qmhd_batch* batch, const int* ctas_per_sm) {
+  return guarded([&] {
+    need(batch);
+    need(ctas_per_sm);
+    batch->impl->set_tuning(std::vector<int>(ctas_per_sm, ctas_per_sm + QMHD_BATCH_PHASES));
+  });
+}
+
+long long qmhd_batch_zones(const qmhd_batch* batch) { return batch ? batch->impl->zones() : -1; }
+
+static_assert(QMHD_BATCH_PHASES == qb::kBpCount, "phase count");
 
 // Allocation-free totals over caller-owned device arrays: validation, the
 // once-per-device scratch lookup, then the two reductions.  Returns codes

@@ -137,9 +137,9 @@ __device__ __forceinline__ void ghost_src(int n, int layer, bool lo, int mode, i
 
 // axis 0: the x sides (both), all padded rows; axis 1: the y sides over all
 // padded columns (run after axis 0 so the corner blocks close last).
-__global__ void k_fill_ghosts(Grid g, StateP u, int axis) {
+__device__ __forceinline__ void b_fill_ghosts(const Grid& g, const StateP& u, int axis, int bx) {
   const int lines = (axis == 0 ? g.ny : g.nx) + 2 * g.ng;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = bx * blockDim.x + threadIdx.x;
   if (t >= 2 * g.ng * lines) return;
   const int side = t / (g.ng * lines);
   const int rem = t - side * g.ng * lines;
@@ -179,6 +179,10 @@ __global__ void k_fill_ghosts(Grid g, StateP u, int axis) {
   } else {
     bn[kd] = sn * bn[ks];
   }
+}
+
+__global__ void k_fill_ghosts(Grid g, StateP u, int axis) {
+  b_fill_ghosts(g, u, axis, blockIdx.x);
 }
 
 // ---- admissible convex fraction (mhd_reduce.hip:120-209) ------------------
@@ -235,10 +239,11 @@ __device__ __forceinline__ double ulp_of(double x) {
 // live-state preflights.  theta_mask: bit0 collocation order 0, bit1 order 1,
 // bit2 order 1 only when the live state's low-order anchor is admissible.
 template <int W>
-__global__ void k_colloc_check(Grid g, StateP cand, StateP base, int has_base, int theta_mask,
-                               int live_checks, int solver_owned, double gamma, Ctl* ctl) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - g.ng;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y - g.ng;
+__device__ __forceinline__ void b_colloc_check(const Grid& g, const StateP& cand, const StateP& base, int has_base,
+                                               int theta_mask, int live_checks, int solver_owned,
+                                               double gamma, Ctl* ctl, int bx, int by) {
+  const int i = bx * blockDim.x + threadIdx.x - g.ng;
+  const int j = by * blockDim.y + threadIdx.y - g.ng;
   if (i >= g.nx + g.ng || j >= g.ny + g.ng) return;
   if (ctl->status & ~kStatusDone) return;
   const long long k = g.idx(i, j);
@@ -298,6 +303,13 @@ __global__ void k_colloc_check(Grid g, StateP cand, StateP base, int has_base, i
       if (scale > 0.0) atomicMax(&ctl->divb_scale, dbits(scale));
     }
   }
+}
+
+template <int W>
+__global__ void k_colloc_check(Grid g, StateP cand, StateP base, int has_base, int theta_mask,
+                               int live_checks, int solver_owned, double gamma, Ctl* ctl) {
+  b_colloc_check<W>(g, cand, base, has_base, theta_mask, live_checks, solver_owned, gamma, ctl, blockIdx.x,
+                    blockIdx.y);
 }
 
 }  // namespace
@@ -617,11 +629,11 @@ __device__ void muscl_pair(const Grid& g, const StateP& u, int i, int j, long lo
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128) k_reconstruct(Grid g, StateP u, IfaceP out, double gamma,
-                                                     const Ctl* ctl) {
+__device__ __forceinline__ void b_reconstruct(const Grid& g, const StateP& u, const IfaceP& out,
+                                              double gamma, const Ctl* ctl, int bx, int by) {
   // dir 0: faces i in [0,nx] over all padded rows; dir 1: transposed.
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - (DIR == 1 ? g.ng : 0);
-  const int j = blockIdx.y * blockDim.y + threadIdx.y - (DIR == 0 ? g.ng : 0);
+  const int i = bx * blockDim.x + threadIdx.x - (DIR == 1 ? g.ng : 0);
+  const int j = by * blockDim.y + threadIdx.y - (DIR == 0 ? g.ng : 0);
   if (DIR == 0 ? (i > g.nx || j >= g.ny + g.ng) : (i >= g.nx + g.ng || j > g.ny)) return;
   if (ctl->status & ~kStatusDone) return;
   const long long k0 = g.idx(i, j);
@@ -661,6 +673,12 @@ __global__ void __launch_bounds__(128) k_reconstruct(Grid g, StateP u, IfaceP ou
     out.L[c][k0] = comp(ul, c);
     out.R[c][k0] = comp(ur, c);
   }
+}
+
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128) k_reconstruct(Grid g, StateP u, IfaceP out, double gamma,
+                                                     const Ctl* ctl) {
+  b_reconstruct<DIR, ORDER>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y);
 }
 
 
@@ -846,15 +864,15 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
 namespace {
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128, 4) k_face_flux_q(Grid g, IfaceP in, FluxP out, double* emf,
-                                                     int* nj, double* spd, double gamma,
-                                                     const Ctl* ctl) {
+__device__ __forceinline__ void b_face_flux_q(const Grid& g, const IfaceP& in, const FluxP& out,
+                                              double* emf, int* nj, double* spd, double gamma,
+                                              const Ctl* ctl, int bx, int by) {
   constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
   constexpr bool kLF = false;
   const int lane = threadIdx.x & 3;
   const unsigned gmask = 0xFu << (threadIdx.x & 28);
-  const int i = blockIdx.x * 32 + (threadIdx.x >> 2);
-  const int j = blockIdx.y;
+  const int i = bx * 32 + (threadIdx.x >> 2);
+  const int j = by;
   if (i > g.nx || j > g.ny) return;  // whole four-lane groups leave together
   if (ctl->status) return;
   int si = i, sj = j;
@@ -948,6 +966,13 @@ __global__ void __launch_bounds__(128, 4) k_face_flux_q(Grid g, IfaceP in, FluxP
   }
   const unsigned nproof = (__ballot_sync(gmask, proof == 0) >> (threadIdx.x & 28)) & 0xFu;
   if (lane == 0) nj[k] = nproof == 0 ? 1 : 0;
+}
+
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128, 4) k_face_flux_q(Grid g, IfaceP in, FluxP out, double* emf,
+                                                     int* nj, double* spd, double gamma,
+                                                     const Ctl* ctl) {
+  b_face_flux_q<DIR, ORDER>(g, in, out, emf, nj, spd, gamma, ctl, blockIdx.x, blockIdx.y);
 }
 
 }  // namespace
@@ -1057,9 +1082,9 @@ constexpr int cell_smem_doubles() {
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(256) k_cell_emf_s(Grid g, StateP u, double* cell_ez,
-                                                    const double* xs, const double* ys,
-                                                    int cfl_reduce, double gamma, Ctl* ctl) {
+__device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, double* cell_ez,
+                                             const double* xs, const double* ys, int cfl_reduce,
+                                             double gamma, Ctl* ctl, int bx, int by) {
   constexpr int H = ORDER == 7 ? 3 : 2, N = 2 * H + 1, Q = ORDER == 7 ? 4 : 3;
   constexpr int TX = kCellTX, TY = kCellTY, SX = TX + 2 * H, SY = TY + 2 * H;
   extern __shared__ double sm[];
@@ -1071,7 +1096,7 @@ __global__ void __launch_bounds__(256) k_cell_emf_s(Grid g, StateP u, double* ce
   if (tid == 0) s_stop = ctl->status;
   __syncthreads();
   if (s_stop) return;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i0 = bx * TX, j0 = by * TY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
@@ -1151,6 +1176,13 @@ __global__ void __launch_bounds__(256) k_cell_emf_s(Grid g, StateP u, double* ce
     for (int w = 1; w < 8; ++w) m = fmax(m, s_max[w]);
     atomicMax(&ctl->max_rate, dbits(m));
   }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(256) k_cell_emf_s(Grid g, StateP u, double* cell_ez,
+                                                    const double* xs, const double* ys,
+                                                    int cfl_reduce, double gamma, Ctl* ctl) {
+  b_cell_emf_s<ORDER>(g, u, cell_ez, xs, ys, cfl_reduce, gamma, ctl, blockIdx.x, blockIdx.y);
 }
 
 // Face -> edge interpolation (mhd_ct.hip:50-97) with the constant shortcut.
@@ -1245,17 +1277,16 @@ __global__ void __launch_bounds__(128) k_corner_emf(Grid g, const double* cell_e
 // through face_index like every CT table read, which keeps them inside the
 // padded grid for any block position.
 template <int ORDER>
-__global__ void __launch_bounds__(128, 4) k_corner_emf_s(Grid g, const double* cell_ez,
-                                                      const double* xemf, const double* yemf,
-                                                      const int* xnj, const int* ynj, double* ez,
-                                                      const Ctl* ctl) {
+__device__ __forceinline__ void b_corner_emf_s(const Grid& g, const double* cell_ez, const double* xemf,
+                                               const double* yemf, const int* xnj, const int* ynj,
+                                               double* ez, const Ctl* ctl, int bx, int by) {
   constexpr int LO = ORDER >= 7 ? -4 : ORDER >= 5 ? -3 : -1;
   constexpr int NT = ORDER >= 7 ? 8 : ORDER >= 5 ? 6 : 2;
   constexpr int TW = 32 + NT - 1, TH = 4 + NT - 1;
   __shared__ double tile[TH][TW];
   if (ctl->status) return;  // uniform over the block
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
-  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 4;
+  const int i0 = bx * 32, j0 = by * 4;
   for (int t = tid; t < TH * TW; t += 128) {
     const int a = t % TW, b = t / TW;
     const int mi = face_index(i0 + LO + a, g.nx, g.bc[0], g.bc[1]);
@@ -1316,15 +1347,23 @@ __global__ void __launch_bounds__(128, 4) k_corner_emf_s(Grid g, const double* c
   ez[k] = v;
 }
 
+template <int ORDER>
+__global__ void __launch_bounds__(128, 4) k_corner_emf_s(Grid g, const double* cell_ez,
+                                                      const double* xemf, const double* yemf,
+                                                      const int* xnj, const int* ynj, double* ez,
+                                                      const Ctl* ctl) {
+  b_corner_emf_s<ORDER>(g, cell_ez, xemf, yemf, xnj, ynj, ez, ctl, blockIdx.x, blockIdx.y);
+}
+
 // Flux difference + EMF curl + Shu-Osher combine (mhd_update.hip:21-206,
 // mhd_ct.hip:893-931, mhd_solver.cpp:840-874).  Writes cells and the owned
 // high faces of the output; ghosts are closed by fill_ghosts afterwards.
-__global__ void __launch_bounds__(256) k_update(Grid g, StateP un, StateP us, StateP out,
-                                                FluxP fx, FluxP fy, const double* ez,
-                                                const double* dt_dev, double dt_host, int stage,
-                                                const Ctl* ctl) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void b_update(const Grid& g, const StateP& un, const StateP& us,
+                                         const StateP& out, const FluxP& fx, const FluxP& fy,
+                                         const double* ez, const double* dt_dev, double dt_host,
+                                         int stage, const Ctl* ctl, int bx, int by) {
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
   if (i > g.nx || j > g.ny) return;
   if (ctl->status) return;
   const double dt = dt_dev ? *dt_dev : dt_host;
@@ -1364,11 +1403,18 @@ __global__ void __launch_bounds__(256) k_update(Grid g, StateP un, StateP us, St
   }
 }
 
+__global__ void __launch_bounds__(256) k_update(Grid g, StateP un, StateP us, StateP out,
+                                                FluxP fx, FluxP fy, const double* ez,
+                                                const double* dt_dev, double dt_host, int stage,
+                                                const Ctl* ctl) {
+  b_update(g, un, us, out, fx, fy, ez, dt_dev, dt_host, stage, ctl, blockIdx.x, blockIdx.y);
+}
+
 // Consume the live-state preflights computed with the previous state and
 // reset the per-step reductions.  coll selects which collocation the
 // admissibility preflight uses (mhd_solver.cpp:689-692); anchor_mode >= 0
 // forces the low-order anchor flag, -1 derives it from the live state.
-__global__ void k_step_begin(Ctl* ctl, int coll, int anchor_mode) {
+__device__ __forceinline__ void k_step_begin_body(Ctl* ctl, int coll, int anchor_mode) {
   if (ctl->status) return;
   int st = 0;
   if ((coll ? ctl->anchor_theta : ctl->live_theta) != dbits(1.0)) st |= kStatusNotAdmissible;
@@ -1385,6 +1431,7 @@ __global__ void k_step_begin(Ctl* ctl, int coll, int anchor_mode) {
   ctl->divb_res = 0ull;
   ctl->divb_scale = 0ull;
 }
+__global__ void k_step_begin(Ctl* ctl, int coll, int anchor_mode) { k_step_begin_body(ctl, coll, anchor_mode); }
 
 // Clear the status word and the live-state accumulators before the live
 // state's preflights are recomputed.
@@ -1396,16 +1443,17 @@ __global__ void k_reset_stats(Ctl* ctl) {
   ctl->divb_scale = 0ull;
 }
 
-__global__ void k_set_time(Ctl* ctl, double t, double t_end) {
+__device__ __forceinline__ void k_set_time_body(Ctl* ctl, double t, double t_end) {
   ctl->t = t;
   ctl->t_end = t_end;
   ctl->steps_done = 0;
   ctl->status = 0;
 }
+__global__ void k_set_time(Ctl* ctl, double t, double t_end) { k_set_time_body(ctl, t, t_end); }
 
 // dt = cfl_eff / max_rate (mhd_solver.cpp:1283-1320), optionally clipped to
 // the remaining interval of a device-resident run.
-__global__ void k_dt(Ctl* ctl, double cfl_eff, double hmin, double hmax, int clip) {
+__device__ __forceinline__ void k_dt_body(Ctl* ctl, double cfl_eff, double hmin, double hmax, int clip) {
   if (ctl->status) return;
   const double mr = __longlong_as_double((long long)ctl->max_rate);
   if (!isfinite(mr)) {
@@ -1423,14 +1471,16 @@ __global__ void k_dt(Ctl* ctl, double cfl_eff, double hmin, double hmax, int cli
   }
   ctl->dt = dt;
 }
+__global__ void k_dt(Ctl* ctl, double cfl_eff, double hmin, double hmax, int clip) { k_dt_body(ctl, cfl_eff, hmin, hmax, clip); }
 
-__global__ void k_step_end(Ctl* ctl) {
+__device__ __forceinline__ void k_step_end_body(Ctl* ctl) {
   if (ctl->status) return;
   const double rem = ctl->t_end - ctl->t;
   ctl->t = ctl->dt == rem ? ctl->t_end : ctl->t + ctl->dt;
   ctl->steps_done += 1;
   if (!(ctl->t < ctl->t_end)) ctl->status |= kStatusDone;
 }
+__global__ void k_step_end(Ctl* ctl) { k_step_end_body(ctl); }
 
 __global__ void k_divb_linf(Grid g, StateP u, unsigned long long* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1477,6 +1527,128 @@ __global__ void k_cell_sums(Grid g, StateP u, double* partial) {
     partial[4 * blockIdx.x + 2] = a[1];
     partial[4 * blockIdx.x + 3] = ca[1];
   }
+}
+
+}  // namespace
+
+// ===========================================================================
+// Batched persistent kernels: each CTA walks the phase's tile list over all
+// instances (stride gridDim.x), decodes (instance, tile) from the prefix
+// table and runs the same device body as the single-instance kernel.
+// ===========================================================================
+namespace {
+
+__device__ __forceinline__ int batch_locate(const BatchPlan& p, int t, int* local) {
+  int lo = 0, hi = p.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(p.prefix + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  *local = t - __ldg(p.prefix + lo);
+  return lo;
+}
+
+__device__ __forceinline__ void batch_block(int phase, const Grid& g, int local, int* bx, int* by) {
+  int tx, ty;
+  batch_tiles(phase, g, &tx, &ty);
+  *bx = local % tx;
+  *by = local / tx;
+}
+
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128) kb_reconstruct(const BatchRec* __restrict__ r, BatchPlan p) {
+  for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
+    int local, bx, by;
+    const BatchRec& q = r[batch_locate(p, t, &local)];
+    batch_block(DIR == 0 ? kBpRecon0 : kBpRecon1, q.a.g, local, &bx, &by);
+    b_reconstruct<DIR, ORDER>(q.a.g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma, q.a.ctl, bx,
+                              by);
+  }
+}
+
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128, 4) kb_face_flux_q(const BatchRec* __restrict__ r,
+                                                         BatchPlan p, int speeds) {
+  for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
+    int local, bx, by;
+    const BatchRec& q = r[batch_locate(p, t, &local)];
+    batch_block(kBpFlux, q.a.g, local, &bx, &by);
+    b_face_flux_q<DIR, ORDER>(q.a.g, DIR == 0 ? q.a.ix : q.a.iy, DIR == 0 ? q.a.fx : q.a.fy,
+                              DIR == 0 ? q.a.xemf : q.a.yemf, DIR == 0 ? q.a.xnj : q.a.ynj,
+                              speeds ? (DIR == 0 ? q.a.xspd : q.a.yspd) : nullptr, q.a.gamma,
+                              q.a.ctl, bx, by);
+  }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(256) kb_cell_emf_s(const BatchRec* __restrict__ r, BatchPlan p,
+                                                     int cfl_reduce) {
+  for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
+    int local, bx, by;
+    const BatchRec& q = r[batch_locate(p, t, &local)];
+    batch_block(kBpCell, q.a.g, local, &bx, &by);
+    b_cell_emf_s<ORDER>(q.a.g, q.a.u, q.a.cell_ez, q.a.xspd, q.a.yspd, cfl_reduce, q.a.gamma,
+                        q.a.ctl, bx, by);
+    __syncthreads();  // shared tiles are reused by the next tile
+  }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128, 4) kb_corner_emf_s(const BatchRec* __restrict__ r,
+                                                          BatchPlan p) {
+  for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
+    int local, bx, by;
+    const BatchRec& q = r[batch_locate(p, t, &local)];
+    batch_block(kBpCorner, q.a.g, local, &bx, &by);
+    b_corner_emf_s<ORDER>(q.a.g, q.a.cell_ez, q.a.xemf, q.a.yemf, q.a.xnj, q.a.ynj, q.a.ez,
+                          q.a.ctl, bx, by);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) kb_update(const BatchRec* __restrict__ r, BatchPlan p,
+                                                 int stage) {
+  for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
+    int local, bx, by;
+    const BatchRec& q = r[batch_locate(p, t, &local)];
+    batch_block(kBpUpdate, q.a.g, local, &bx, &by);
+    b_update(q.a.g, q.live, q.a.u, q.out, q.a.fx, q.a.fy, q.a.ez, &q.a.ctl->dt, 0.0, stage,
+             q.a.ctl, bx, by);
+  }
+}
+
+__global__ void __launch_bounds__(256) kb_fill_ghosts(const BatchRec* __restrict__ r, BatchPlan p,
+                                                      int axis) {
+  for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
+    int local;
+    const BatchRec& q = r[batch_locate(p, t, &local)];
+    b_fill_ghosts(q.a.g, q.out, axis, local);
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) kb_colloc_check(const BatchRec* __restrict__ r,
+                                                       BatchPlan p, int theta_mask,
+                                                       int live_checks) {
+  for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
+    int local, bx, by;
+    const BatchRec& q = r[batch_locate(p, t, &local)];
+    batch_block(kBpColloc, q.a.g, local, &bx, &by);
+    b_colloc_check<W>(q.a.g, q.out, q.live, 1, theta_mask, live_checks, 1, q.a.gamma, q.a.ctl,
+                      bx, by);
+  }
+}
+
+__global__ void kb_ctl(const BatchRec* __restrict__ r, int n, int what, double t0, double t_end) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const BatchRec& q = r[k];
+  Ctl* ctl = q.a.ctl;
+  if (what == 0) k_step_begin_body(ctl, 0, -1);
+  else if (what == 1) k_dt_body(ctl, q.cfl_eff, q.hmin, q.hmax, 1);
+  else if (what == 2) k_step_end_body(ctl);
+  else k_set_time_body(ctl, t0, t_end);
 }
 
 }  // namespace
@@ -1633,6 +1805,117 @@ void launch_divb_linf(const Grid& g, const StateP& u, unsigned long long* out, c
 
 void launch_cell_sums(const Grid& g, const StateP& u, double* partial, int blocks, cudaStream_t s) {
   k_cell_sums<<<blocks, 256, 0, s>>>(g, u, partial);
+}
+
+// ---- batched launchers -----------------------------------------------------
+namespace {
+template <class K>
+int max_ctas(K kernel, int threads, size_t smem) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem) != cudaSuccess) b = 1;
+  return b > 0 ? b : 1;
+}
+inline unsigned pgrid(const BatchPlan& p) { return unsigned(p.grid > 0 ? p.grid : p.total); }
+
+template <int ORDER>
+void batch_cell_configure() {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(kb_cell_emf_s<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(sizeof(double) * cell_smem_doubles<ORDER>()));
+    done = true;
+  }
+}
+}  // namespace
+
+int batch_phase_threads(int phase) {
+  switch (phase) {
+    case kBpRecon0: case kBpRecon1: case kBpFlux: case kBpCorner: return 128;
+    default: return 256;
+  }
+}
+
+int batch_phase_max_ctas_per_sm(int phase, int order) {
+  const bool o7 = order == 7;
+  switch (phase) {
+    case kBpRecon0: return o7 ? max_ctas(kb_reconstruct<0, 7>, 128, 0) : max_ctas(kb_reconstruct<0, 5>, 128, 0);
+    case kBpRecon1: return o7 ? max_ctas(kb_reconstruct<1, 7>, 128, 0) : max_ctas(kb_reconstruct<1, 5>, 128, 0);
+    case kBpFlux: return o7 ? max_ctas(kb_face_flux_q<0, 7>, 128, 0) : max_ctas(kb_face_flux_q<0, 5>, 128, 0);
+    case kBpCell:
+      if (o7) {
+        batch_cell_configure<7>();
+        return max_ctas(kb_cell_emf_s<7>, 256, sizeof(double) * cell_smem_doubles<7>());
+      }
+      batch_cell_configure<5>();
+      return max_ctas(kb_cell_emf_s<5>, 256, sizeof(double) * cell_smem_doubles<5>());
+    case kBpCorner: return o7 ? max_ctas(kb_corner_emf_s<7>, 128, 0) : max_ctas(kb_corner_emf_s<5>, 128, 0);
+    case kBpUpdate: return max_ctas(kb_update, 256, 0);
+    case kBpColloc: return o7 ? max_ctas(kb_colloc_check<8>, 256, 0) : max_ctas(kb_colloc_check<6>, 256, 0);
+    default: return max_ctas(kb_fill_ghosts, 256, 0);
+  }
+}
+
+void launch_batch_reconstruct(const BatchRec* r, const BatchPlan& p, int dir, int order,
+                              cudaStream_t s) {
+  const dim3 block(32, 4);
+  if (order == 7) {
+    if (dir == 0) kb_reconstruct<0, 7><<<pgrid(p), block, 0, s>>>(r, p);
+    else kb_reconstruct<1, 7><<<pgrid(p), block, 0, s>>>(r, p);
+  } else {
+    if (dir == 0) kb_reconstruct<0, 5><<<pgrid(p), block, 0, s>>>(r, p);
+    else kb_reconstruct<1, 5><<<pgrid(p), block, 0, s>>>(r, p);
+  }
+}
+
+void launch_batch_face_flux(const BatchRec* r, const BatchPlan& p, int dir, int order,
+                            bool speeds, cudaStream_t s) {
+  const int sp = speeds ? 1 : 0;
+  if (order == 7) {
+    if (dir == 0) kb_face_flux_q<0, 7><<<pgrid(p), 128, 0, s>>>(r, p, sp);
+    else kb_face_flux_q<1, 7><<<pgrid(p), 128, 0, s>>>(r, p, sp);
+  } else {
+    if (dir == 0) kb_face_flux_q<0, 5><<<pgrid(p), 128, 0, s>>>(r, p, sp);
+    else kb_face_flux_q<1, 5><<<pgrid(p), 128, 0, s>>>(r, p, sp);
+  }
+}
+
+void launch_batch_cell_emf(const BatchRec* r, const BatchPlan& p, int order, bool cfl_reduce,
+                           cudaStream_t s) {
+  const dim3 block(kCellTX, kCellTY);
+  if (order == 7) {
+    batch_cell_configure<7>();
+    kb_cell_emf_s<7><<<pgrid(p), block, sizeof(double) * cell_smem_doubles<7>(), s>>>(
+        r, p, cfl_reduce ? 1 : 0);
+  } else {
+    batch_cell_configure<5>();
+    kb_cell_emf_s<5><<<pgrid(p), block, sizeof(double) * cell_smem_doubles<5>(), s>>>(
+        r, p, cfl_reduce ? 1 : 0);
+  }
+}
+
+void launch_batch_corner_emf(const BatchRec* r, const BatchPlan& p, int order, cudaStream_t s) {
+  const dim3 block(32, 4);
+  if (order == 7) kb_corner_emf_s<7><<<pgrid(p), block, 0, s>>>(r, p);
+  else kb_corner_emf_s<5><<<pgrid(p), block, 0, s>>>(r, p);
+}
+
+void launch_batch_update(const BatchRec* r, const BatchPlan& p, int stage, cudaStream_t s) {
+  kb_update<<<pgrid(p), dim3(32, 8), 0, s>>>(r, p, stage);
+}
+
+void launch_batch_fill_ghosts(const BatchRec* r, const BatchPlan& p, int axis, cudaStream_t s) {
+  kb_fill_ghosts<<<pgrid(p), 256, 0, s>>>(r, p, axis);
+}
+
+void launch_batch_colloc_check(const BatchRec* r, const BatchPlan& p, int order, int theta_mask,
+                               bool live_checks, cudaStream_t s) {
+  const dim3 block(32, 8);
+  if (order == 7) kb_colloc_check<8><<<pgrid(p), block, 0, s>>>(r, p, theta_mask, live_checks ? 1 : 0);
+  else kb_colloc_check<6><<<pgrid(p), block, 0, s>>>(r, p, theta_mask, live_checks ? 1 : 0);
+}
+
+void launch_batch_ctl(const BatchRec* r, int n, int what, double t, double t_end, cudaStream_t s) {
+  kb_ctl<<<cdiv(n, 128), 128, 0, s>>>(r, n, what, t, t_end);
 }
 
 }  // namespace qb

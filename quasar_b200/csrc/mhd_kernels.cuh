@@ -111,4 +111,68 @@ void launch_divb_linf(const Grid& g, const StateP& u, unsigned long long* out, c
 void launch_cell_sums(const Grid& g, const StateP& u, double* partial, int blocks,
                       cudaStream_t s);
 
+// ---- batched step: many independent instances per launch -----------------
+// One record per instance and stage: the instance's stage arguments (a.u is
+// the stage input), its live register (update and admissibility base) and the
+// stage's output register, plus its dt parameters.
+struct BatchRec {
+  StageArgs a;
+  StateP live, out;
+  double cfl_eff, hmin, hmax;
+};
+
+// Tile phases of a batched stage.  A phase's prefix table maps a global tile
+// index to (instance, tile within the instance): prefix[i] is the first tile
+// of instance i, prefix[n] the total.
+enum BatchPhase : int {
+  kBpRecon0, kBpRecon1, kBpFlux, kBpCell, kBpCorner, kBpUpdate, kBpColloc, kBpFill0, kBpFill1,
+  kBpCount
+};
+struct BatchPlan {
+  const int* prefix;  // device, n + 1 entries
+  int n;              // instances
+  int total;          // tiles over all instances
+  int grid;           // CTAs of the persistent launch (<= total)
+};
+
+// Tiles of one instance in a phase (x count, y count); the same function
+// drives the host plans and the device tile decode.
+__host__ __device__ inline void batch_tiles(int phase, const Grid& g, int* tx, int* ty) {
+  auto cd = [](int a, int b) { return (a + b - 1) / b; };
+  switch (phase) {
+    case kBpRecon0: *tx = cd(g.nx + 1, 32); *ty = cd(g.ny + 2 * g.ng, 4); break;
+    case kBpRecon1: *tx = cd(g.nx + 2 * g.ng, 32); *ty = cd(g.ny + 1, 4); break;
+    case kBpFlux: *tx = cd(g.nx + 1, 32); *ty = g.ny + 1; break;
+    case kBpCell: *tx = cd(g.nx + 1, 32); *ty = cd(g.ny + 1, 8); break;
+    case kBpCorner: *tx = cd(g.nx + 1, 32); *ty = cd(g.ny + 1, 4); break;
+    case kBpUpdate: *tx = cd(g.nx + 1, 32); *ty = cd(g.ny + 1, 8); break;
+    case kBpColloc: *tx = cd(g.nx + 2 * g.ng, 32); *ty = cd(g.ny + 2 * g.ng, 8); break;
+    case kBpFill0: *tx = cd(2 * g.ng * (g.ny + 2 * g.ng), 256); *ty = 1; break;
+    default: *tx = cd(2 * g.ng * (g.nx + 2 * g.ng), 256); *ty = 1; break;
+  }
+}
+
+// Threads per CTA of each phase's batched kernel and its resident CTAs per SM
+// (queried once per process), for sizing persistent grids.
+int batch_phase_threads(int phase);
+int batch_phase_max_ctas_per_sm(int phase, int order);
+
+// Batched launches: every record's instance in one persistent launch.  Records
+// are indexed like the plan's prefix table.  All instances share `order`.
+void launch_batch_reconstruct(const BatchRec* r, const BatchPlan& p, int dir, int order,
+                              cudaStream_t s);
+void launch_batch_face_flux(const BatchRec* r, const BatchPlan& p, int dir, int order,
+                            bool speeds, cudaStream_t s);
+void launch_batch_cell_emf(const BatchRec* r, const BatchPlan& p, int order, bool cfl_reduce,
+                           cudaStream_t s);
+void launch_batch_corner_emf(const BatchRec* r, const BatchPlan& p, int order, cudaStream_t s);
+void launch_batch_update(const BatchRec* r, const BatchPlan& p, int stage, cudaStream_t s);
+void launch_batch_fill_ghosts(const BatchRec* r, const BatchPlan& p, int axis, cudaStream_t s);
+void launch_batch_colloc_check(const BatchRec* r, const BatchPlan& p, int order, int theta_mask,
+                               bool live_checks, cudaStream_t s);
+// Per-instance control kernels (one thread per instance): 0 step_begin
+// (collocation 0, anchor from the live state), 1 dt (clipped to t_end),
+// 2 step_end, 3 set_time(t, t_end).
+void launch_batch_ctl(const BatchRec* r, int n, int what, double t, double t_end, cudaStream_t s);
+
 }  // namespace qb

@@ -31,6 +31,8 @@ struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
+class MhdBatch2D;
+
 class MhdSolver2D {
  public:
   explicit MhdSolver2D(const Config& cfg);
@@ -72,6 +74,7 @@ class MhdSolver2D {
   cudaStream_t stream() const { return stream_; }
 
  private:
+  friend class MhdBatch2D;  // batched stage launches over the same registers
   struct Attempt {
     bool ok;
     double theta;

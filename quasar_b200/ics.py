@@ -47,11 +47,12 @@ def orszag_tang(n, order=5, gamma=5.0 / 3.0, amplitude=1.0, ny=None):
                      -b0 * np.sin(2 * pi * Y), b0 * np.sin(4 * pi * X), z, gamma)
 
 
-def rotor(n, order=7, gamma=5.0 / 3.0):
+def rotor(n, order=7, gamma=5.0 / 3.0, ny=None):
     """rho=10 for r<0.1, linear taper to 1 at r=0.115, rigid rotation u0=2 at
     r0=0.1 tapering to rest at r1, p=1, Bx=5/sqrt(4 pi) (mhd_initial_conditions.hip:159-188)."""
     ng = nghost(order)
-    X, Y = np.meshgrid(_centres(n, ng), _centres(n, ng), indexing="xy")
+    ny = n if ny is None else ny
+    X, Y = np.meshgrid(_centres(n, ng), _centres(ny, ng), indexing="xy")
     rx, ry = X - 0.5, Y - 0.5
     r = np.hypot(rx, ry)
     r0, r1, u0 = 0.1, 0.115, 2.0
@@ -64,10 +65,11 @@ def rotor(n, order=7, gamma=5.0 / 3.0):
                      np.full_like(X, 5.0 / math.sqrt(4.0 * math.pi)), z, z, gamma)
 
 
-def blast(n, order=7, gamma=5.0 / 3.0):
+def blast(n, order=7, gamma=5.0 / 3.0, ny=None):
     """p=100 for r<0.1 else 0.1, rho=1, Bx=By=10/sqrt(8 pi) (mhd_initial_conditions.hip:145-157)."""
     ng = nghost(order)
-    X, Y = np.meshgrid(_centres(n, ng), _centres(n, ng), indexing="xy")
+    ny = n if ny is None else ny
+    X, Y = np.meshgrid(_centres(n, ng), _centres(ny, ng), indexing="xy")
     r = np.hypot(X - 0.5, Y - 0.5)
     b = 10.0 / math.sqrt(8.0 * math.pi)
     z = np.zeros_like(X)
@@ -75,4 +77,221 @@ def blast(n, order=7, gamma=5.0 / 3.0):
                      np.full_like(X, b), np.full_like(X, b), z, gamma)
 
 
+# ---- families without a reference generator --------------------------------
+# The reference's Brio-Wu tube is x-aligned and its Alfven wave x-propagating
+# (mhd_initial_conditions.hip:67-114).  Oblique versions take the in-plane
+# field from a corner vector potential A_z (B = curl A, the stencil of
+# launch_mhd_curl_corner_potential, physics/mhd/kernels.hpp:725-728).  A
+# seeded field must be discretely divergence-free to the bit (mhd_solver.cpp
+# 1196-1222 accepts round-off only where both derivatives cancel), so the
+# field is built on an exact lattice: cells of side h = 2^-9, the periodic
+# part of A rounded to multiples of q = h 2^-35 on the periodic corner
+# lattice and the uniform part rounded to multiples of 2^-35.  Every face
+# value, face difference and divided difference is then exact in binary64
+# and the discrete divergence is exactly zero.
+
+_F2C = {6: ([11, -93, 802, 802, -93, 11], 1440.0),
+        8: ([-191, 1879, -9531, 68323, 68323, -9531, 1879, -191], 120960.0),
+        4: ([-1, 13, 13, -1], 24.0)}
+
+
+def _collocate(face, axis, ng):
+    """Cell values of a face field by the centred face -> cell rational
+    stencil (mhd_staggering.hpp:77-112) where it fits in the padded array;
+    NaN elsewhere."""
+    w, den = _F2C[2 * ng]
+    W = len(w)
+    out = np.full_like(face, np.nan)
+    n = face.shape[1 - axis]
+    for c in range(W // 2 - 1, n - W // 2):
+        acc = 0.0
+        for k in range(W):
+            q = c - (W // 2 - 1) + k
+            acc = acc + w[k] * (face[:, q] if axis == 0 else face[q, :])
+        if axis == 0:
+            out[:, c] = acc / den
+        else:
+            out[c, :] = acc / den
+    return out
+
+
+def _assemble_faces(rho, vx, vy, vz, p, bx_face, by_face, bz, gamma, ng):
+    """Conserved arrays with the face field; the magnetic energy uses the
+    collocated cell field the solver itself reads back, so that the gas
+    pressure is the intended p (the reference recollocates the magnetic
+    energy when seeding, mhd_initial_conditions.hip:222-340)."""
+    bxc = _collocate(bx_face, 0, ng)
+    byc = _collocate(by_face, 1, ng)
+    kin = 0.5 * rho * (vx * vx + vy * vy + vz * vz)
+    mag = 0.5 * (bxc * bxc + byc * byc + bz * bz)
+    near = 0.5 * (0.25 * (bx_face + np.roll(bx_face, -1, 1)) ** 2 +
+                  0.25 * (by_face + np.roll(by_face, -1, 0)) ** 2 + bz * bz)
+    energy = p / (gamma - 1.0) + kin + np.where(np.isfinite(mag), mag, near)
+    return [np.ascontiguousarray(a, dtype=np.float64) for a in
+            (rho, rho * vx, rho * vy, rho * vz, energy, bx_face, by_face, bz)]
+
+
+OBLIQUE_H = 2.0 ** -9
+_QB = 2.0 ** -35  # lattice of field values
+
+
+def _lattice_faces(a, b, Ap, nx, ny, ng, h=OBLIQUE_H):
+    """Faces of B = (b, -a) + curl(Ap z) with Ap periodic on the box
+    (nx h) x (ny h): Ap is sampled at the wrapped corner positions."""
+    ii = np.arange(-ng, nx + ng + 1)
+    jj = np.arange(-ng, ny + ng + 1)
+    XC, YC = np.meshgrid((ii % nx) * h, (jj % ny) * h, indexing="xy")
+    A = np.rint(Ap(XC, YC) / (_QB * h))  # integer multiples of q
+    bq = float(np.rint(b / _QB)) * _QB
+    aq = float(np.rint(a / _QB)) * _QB
+    bx = bq + (A[1:, :-1] - A[:-1, :-1]) * _QB
+    by = -aq - (A[:-1, 1:] - A[:-1, :-1]) * _QB
+    return np.ascontiguousarray(bx), np.ascontiguousarray(by)
+
+
+def oblique_modes(angle, lx, ly, kmax=4):
+    """Wave numbers (l, m) along x and y, 0..kmax, whose direction
+    atan2(m/ly, l/lx) is closest to `angle`; the pattern is then periodic."""
+    best = None
+    for l in range(kmax + 1):
+        for m in range(kmax + 1):
+            if l == 0 and m == 0:
+                continue
+            th = math.atan2(m / ly, l / lx)
+            d = abs(th - angle)
+            if best is None or d < best[0] - 1e-12:
+                best = (d, l, m)
+    return best[1], best[2]
+
+
+def _oblique_frame(n, ny, angle):
+    lx, ly = n * OBLIQUE_H, ny * OBLIQUE_H
+    l, m = oblique_modes(angle, lx, ly)
+    kx, ky = l / lx, m / ly
+    lam = 1.0 / math.hypot(kx, ky)
+    c, s_ = kx * lam, ky * lam
+    return lx, ly, kx, ky, lam, c, s_
+
+
+def brio_wu_rotated(n, ny=None, order=5, angle=0.0, gamma=2.0, bn=0.75, bt=1.0):
+    """Brio-Wu states (rho 1 | 0.125, p 1 | 0.1, B_n = 0.75, B_t = +1 | -1,
+    gamma 2) as a periodic double shock tube: the left state fills the band
+    1/4 <= frac(phase) < 3/4 of a plane pattern whose normal is the closest
+    commensurate direction to `angle` (oblique_modes) on the exact lattice
+    box (n h) x (ny h).  Outflow ghosts of an oblique tube would copy a field
+    that the cell collocation no longer matches, so the tube is periodic.
+    Returns (arrays, lx, ly, angle used)."""
+    ny = n if ny is None else ny
+    ng = nghost(order)
+    lx, ly, kx, ky, lam, c, s_ = _oblique_frame(n, ny, angle)
+
+    def G(f):  # integral of B_t over the normal coordinate, per unit phase
+        return np.where(f < 0.25, -bt * f,
+                        np.where(f < 0.75, -0.25 * bt + bt * (f - 0.25),
+                                 0.25 * bt - bt * (f - 0.75)))
+
+    def Ap(x, y):
+        ph = kx * x + ky * y
+        return -lam * G(ph - np.floor(ph))
+
+    bx, by = _lattice_faces(-bn * s_, bn * c, Ap, n, ny, ng)
+    X, Y = np.meshgrid(_centres(n, ng, lx), _centres(ny, ng, ly), indexing="xy")
+    ph = kx * X + ky * Y
+    f = ph - np.floor(ph)
+    left = (f >= 0.25) & (f < 0.75)
+    rho = np.where(left, 1.0, 0.125)
+    p = np.where(left, 1.0, 0.1)
+    z = np.zeros_like(X)
+    return (_assemble_faces(rho, z, z, z, p, bx, by, z, gamma, ng), lx, ly,
+            math.atan2(s_, c))
+
+
+def _wave_eigenvector(kind, rho, p, bn, bt1, bt2, gamma):
+    """Right eigenvector of the 1-D primitive Jacobian (rho, vn, vt1, vt2, p,
+    bt1, bt2) at rest for the right-going fast or Alfven wave."""
+    J = np.zeros((7, 7))
+    J[0, 1] = rho
+    J[1, 4], J[1, 5], J[1, 6] = 1.0 / rho, bt1 / rho, bt2 / rho
+    J[2, 5] = -bn / rho
+    J[3, 6] = -bn / rho
+    J[4, 1] = gamma * p
+    J[5, 1], J[5, 2] = bt1, -bn
+    J[6, 1], J[6, 3] = bt2, -bn
+    w, V = np.linalg.eig(J)
+    w, V = w.real, V.real
+    if kind == "fast":
+        k = int(np.argmax(w))
+    else:
+        ca = abs(bn) / math.sqrt(rho)
+        k = int(np.argmin(np.abs(w - ca)))
+    r = V[:, k]
+    return r / np.max(np.abs(r)), float(w[k])
+
+
+def linear_wave(n, ny=None, order=5, angle=math.pi / 4, kind="fast", amplitude=1e-6,
+                gamma=5.0 / 3.0):
+    """Linear fast or Alfven wave, one wavelength per commensurate period of
+    the exact lattice box (n h) x (ny h) along the direction closest to
+    `angle`; background rho=1, p=1/gamma, wave-frame B = (1, sqrt 2, 1/2).
+    Returns (arrays, lx, ly, angle used)."""
+    ny = n if ny is None else ny
+    ng = nghost(order)
+    lx, ly, kx, ky, lam, c, s_ = _oblique_frame(n, ny, angle)
+    rho0, p0, bn, b1, b2 = 1.0, 1.0 / gamma, 1.0, math.sqrt(2.0), 0.5
+    r, _ = _wave_eigenvector(kind, rho0, p0, bn, b1, b2, gamma)
+    two_pi = 2.0 * math.pi
+
+    def Ap(x, y):
+        return -amplitude * r[5] * lam * np.sin(two_pi * (kx * x + ky * y)) / two_pi
+
+    bx, by = _lattice_faces(-bn * s_ - b1 * c, bn * c - b1 * s_, Ap, n, ny, ng)
+    X, Y = np.meshgrid(_centres(n, ng, lx), _centres(ny, ng, ly), indexing="xy")
+    ph = amplitude * np.cos(two_pi * (kx * X + ky * Y))
+    rho = rho0 + r[0] * ph
+    vn, vt1, vt2 = r[1] * ph, r[2] * ph, r[3] * ph
+    p = p0 + r[4] * ph
+    bz = b2 + r[6] * ph
+    vx, vy = vn * c - vt1 * s_, vn * s_ + vt1 * c
+    return (_assemble_faces(rho, vx, vy, vt2, p, bx, by, bz, gamma, ng), lx, ly,
+            math.atan2(s_, c))
+
+
 GENERATORS = {"orszag_tang": orszag_tang, "rotor": rotor, "blast": blast}
+
+
+def batch_instances(count=256, seed=0, lo=64, hi=512, order=5):
+    """The seeded batch of independent instances: sides log-uniform in
+    [lo, hi] per axis; family uniform over Orszag-Tang (amplitude U[0.5, 2],
+    periodic, unit box), rotated Brio-Wu (angle U[0, pi/2), gamma 2, periodic
+    double tube) and a linear fast or Alfven wave (amplitude 1e-6, angle
+    U[0, pi/2), periodic); the oblique families live on the exact lattice box
+    (nx h) x (ny h) with the commensurate direction closest to the drawn
+    angle.
+    Returns dicts with family, nx, ny, lx, ly, gamma, bc (0 periodic,
+    1 outflow) and a zero-argument `arrays` callable."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nx = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        ny = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        fam = int(rng.integers(0, 3))
+        if fam == 0:
+            amp = float(rng.uniform(0.5, 2.0))
+            out.append(dict(family="orszag_tang", nx=nx, ny=ny, lx=1.0, ly=1.0,
+                            gamma=5.0 / 3.0, bc=0, amplitude=amp,
+                            arrays=lambda nx=nx, ny=ny, amp=amp: orszag_tang(
+                                nx, order=order, amplitude=amp, ny=ny)))
+        elif fam == 1:
+            ang = float(rng.uniform(0.0, math.pi / 2))
+            out.append(dict(family="brio_wu", nx=nx, ny=ny, lx=nx * OBLIQUE_H,
+                            ly=ny * OBLIQUE_H, gamma=2.0, bc=0, angle=ang,
+                            arrays=lambda nx=nx, ny=ny, ang=ang: brio_wu_rotated(
+                                nx, ny, order=order, angle=ang)[0]))
+        else:
+            ang = float(rng.uniform(0.0, math.pi / 2))
+            kind = "fast" if rng.integers(0, 2) == 0 else "alfven"
+            out.append(dict(family=f"{kind}_wave", nx=nx, ny=ny, lx=nx * OBLIQUE_H,
+                            ly=ny * OBLIQUE_H, gamma=5.0 / 3.0, bc=0, angle=ang,
+                            arrays=lambda nx=nx, ny=ny, ang=ang, kind=kind: linear_wave(
+                                nx, ny, order=order, angle=ang, kind=kind)[0]))
+    return out

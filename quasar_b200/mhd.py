@@ -115,11 +115,15 @@ def _native_config(cfg: MhdConfig) -> _native.QmhdConfig:
 class MhdSolver2D:
     """physics/mhd/mhd_solver.hpp:85-173 on the sm_100a kernels."""
 
-    def __init__(self, config: MhdConfig):
+    def __init__(self, config: MhdConfig, _handle=None, _owner=None):
         L = _native.lib()
         self._cfg = config
-        h = ctypes.c_void_p()
-        _native.check(L.qmhd_solver_create(ctypes.byref(_native_config(config)), ctypes.byref(h)))
+        self._owner = _owner  # a batch view keeps its batch alive
+        if _handle is None:
+            h = ctypes.c_void_p()
+            _native.check(L.qmhd_solver_create(ctypes.byref(_native_config(config)), ctypes.byref(h)))
+        else:
+            h = _handle
         self._h = h
         nx, ny, ng = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _native.check(L.qmhd_solver_grid(self._h, ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(ng)))
@@ -129,9 +133,9 @@ class MhdSolver2D:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and getattr(self, "_owner", None) is None:
             _native.lib().qmhd_solver_destroy(h)
-            self._h = None
+        self._h = None
 
     def grid(self) -> Grid2D:
         return self._grid
@@ -184,3 +188,63 @@ class MhdSolver2D:
         _native.check(_native.lib().qmhd_solver_advance_auto(
             self._h, ctypes.byref(tt), float(t_end), int(max_steps), ctypes.byref(n)))
         return tt.value, n.value
+
+
+class MhdBatch2D:
+    """Many independent instances stepped together (include/quasar_mhd_batch.h).
+
+    No counterpart in the reference, which runs one MhdSolver2D per instance.
+    `instance(i)` is an MhdSolver2D view of instance i (seed, read, check or
+    step it alone); `advance(steps)` steps every instance with its own auto dt
+    in batched persistent launches replayed as CUDA graphs.
+    """
+
+    PHASES = 9
+
+    def __init__(self, configs):
+        L = _native.lib()
+        configs = list(configs)
+        arr = (_native.QmhdConfig * len(configs))(*[_native_config(c) for c in configs])
+        h = ctypes.c_void_p()
+        _native.check(L.qmhd_batch_create(arr, len(configs), ctypes.byref(h)))
+        self._h = h
+        self._views = [MhdSolver2D(c, _handle=ctypes.c_void_p(L.qmhd_batch_instance(h, i)),
+                                   _owner=self) for i, c in enumerate(configs)]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            for v in getattr(self, "_views", []):
+                v._h = None
+            _native.lib().qmhd_batch_destroy(h)
+            self._h = None
+
+    def __len__(self) -> int:
+        return len(self._views)
+
+    def instance(self, i: int) -> MhdSolver2D:
+        return self._views[i]
+
+    def zones(self) -> int:
+        return int(_native.lib().qmhd_batch_zones(self._h))
+
+    def advance(self, steps: int) -> list:
+        done = (ctypes.c_int * len(self))()
+        _native.check(_native.lib().qmhd_batch_advance(self._h, int(steps), done))
+        return list(done)
+
+    def time_steps(self, steps: int):
+        ms, zu = ctypes.c_double(), ctypes.c_longlong()
+        _native.check(_native.lib().qmhd_batch_time_steps(
+            self._h, int(steps), ctypes.byref(ms), ctypes.byref(zu)))
+        return ms.value, zu.value
+
+    def autotune(self):
+        c = (ctypes.c_int * self.PHASES)()
+        t = ctypes.c_int()
+        _native.check(_native.lib().qmhd_batch_autotune(self._h, c, ctypes.byref(t)))
+        return list(c), t.value
+
+    def set_tuning(self, ctas_per_sm) -> None:
+        c = (ctypes.c_int * self.PHASES)(*[int(x) for x in ctas_per_sm])
+        _native.check(_native.lib().qmhd_batch_set_tuning(self._h, c))

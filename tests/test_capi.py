@@ -27,6 +27,9 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared_symbols() if not hasattr(lib, s)]
     assert not missing, missing
     assert set(declared_symbols()) == set(_native.EXPORTS)
+    batch = declared_symbols("quasar_mhd_batch.h")
+    assert set(batch) == set(_native.BATCH_EXPORTS)
+    assert all(hasattr(lib, s) for s in batch)
     ext = declared_symbols("quasar_mhd_ext.h")
     assert set(ext) == set(_native.EXT_EXPORTS)
     assert all(hasattr(lib, s) for s in ext)
