@@ -29,6 +29,8 @@ TOTALS_DEVICE_MAX_CELLS = 67108864
 BATCH_EXPORTS = ("qmhd_batch_create", "qmhd_batch_destroy", "qmhd_batch_size", "qmhd_batch_zones",
                  "qmhd_batch_instance", "qmhd_batch_advance", "qmhd_batch_time_steps",
                  "qmhd_batch_autotune", "qmhd_batch_set_tuning")
+INDICATOR_EXPORTS = ("qmhd_indicator_create", "qmhd_indicator_destroy", "qmhd_indicator_get_params",
+                     "qmhd_indicator_set_params", "qmhd_indicator_forward")
 
 
 class QmhdConfig(ctypes.Structure):
@@ -89,6 +91,12 @@ def lib() -> ctypes.CDLL:
     L.qmhd_batch_time_steps.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(ctypes.c_longlong)]
     L.qmhd_batch_autotune.argtypes = [vp, ip, ip]
     L.qmhd_batch_set_tuning.argtypes = [vp, ip]
+    L.qmhd_indicator_create.argtypes = [ctypes.c_ulonglong, ctypes.POINTER(vp)]
+    L.qmhd_indicator_destroy.argtypes = [vp]
+    L.qmhd_indicator_destroy.restype = None
+    L.qmhd_indicator_get_params.argtypes = [vp, vp, ctypes.c_size_t]
+    L.qmhd_indicator_set_params.argtypes = [vp, vp, ctypes.c_size_t]
+    L.qmhd_indicator_forward.argtypes = [vp, vp, ctypes.c_longlong, vp]
     _lib = L
     return L
 

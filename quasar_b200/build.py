@@ -21,8 +21,8 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libquasar_mhd_b200.so")
-SOURCES = ["mhd_kernels.cu", "mhd_solver.cu", "mhd_batch.cu", "capi.cu", "probe.cu", "noalloc.cu"]
-HEADERS = ["mhd_device.cuh", "mhd_kernels.cuh", "mhd_solver.cuh", "mhd_batch.cuh", "noalloc.cuh"]
+SOURCES = ["mhd_kernels.cu", "mhd_solver.cu", "mhd_batch.cu", "capi.cu", "probe.cu", "noalloc.cu", "indicator.cu"]
+HEADERS = ["mhd_device.cuh", "mhd_kernels.cuh", "mhd_solver.cuh", "mhd_batch.cuh", "noalloc.cuh", "indicator.cuh", "tc.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-diag-suppress", "177"]

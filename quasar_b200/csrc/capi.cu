@@ -2,6 +2,8 @@
 #include "../../include/quasar_mhd.h"
 #include "../../include/quasar_mhd_ext.h"
 #include "../../include/quasar_mhd_batch.h"
+#include "../../include/quasar_mhd_indicator.h"
+#include "indicator.cuh"
 #include "mhd_batch.cuh"
 #include "mhd_solver.cuh"
 #include "noalloc.cuh"
@@ -23,6 +25,11 @@ double fp64_fma_peak_tflops();
 struct qmhd_solver {
   qb::MhdSolver2D* impl = nullptr;
   bool owned = false;
+};
+
+struct qmhd_indicator {
+  qb::Indicator impl;
+  explicit qmhd_indicator(unsigned long long seed) : impl(seed) {}
 };
 
 struct qmhd_batch {
@@ -295,6 +302,50 @@ int qmhd_batch_set_tuning(qmhd_batch* batch, const int* ctas_per_sm) {
 long long qmhd_batch_zones(const qmhd_batch* batch) { return batch ? batch->impl->zones() : -1; }
 
 static_assert(QMHD_BATCH_PHASES == qb::kBpCount, "phase count");
+
+// ---- learned troubled-cell indicator (include/quasar_mhd_indicator.h) -----
+static_assert(QMHD_INDICATOR_PARAMS == qb::kParamCount, "parameter count");
+
+int qmhd_indicator_create(unsigned long long seed, qmhd_indicator** out) {
+  return guarded([&] {
+    need(out);
+    *out = nullptr;
+    *out = new qmhd_indicator(seed);
+  });
+}
+
+void qmhd_indicator_destroy(qmhd_indicator* ind) { delete ind; }
+
+int qmhd_indicator_get_params(qmhd_indicator* ind, float* params, size_t n) {
+  return guarded([&] {
+    need(ind);
+    need(params);
+    if (n != size_t(QMHD_INDICATOR_PARAMS))
+      throw std::invalid_argument("qmhd_indicator_get_params: need QMHD_INDICATOR_PARAMS floats");
+    ind->impl.get_params(params);
+  });
+}
+
+int qmhd_indicator_set_params(qmhd_indicator* ind, const float* params, size_t n) {
+  return guarded([&] {
+    need(ind);
+    need(params);
+    if (n != size_t(QMHD_INDICATOR_PARAMS))
+      throw std::invalid_argument("qmhd_indicator_set_params: need QMHD_INDICATOR_PARAMS floats");
+    ind->impl.set_params(params);
+  });
+}
+
+int qmhd_indicator_forward(qmhd_indicator* ind, const float* features, long long rows,
+                           float* logits) {
+  return guarded([&] {
+    need(ind);
+    need(features);
+    need(logits);
+    if (rows < 0) throw std::invalid_argument("qmhd_indicator_forward: rows must be >= 0");
+    ind->impl.forward(features, rows, logits);
+  });
+}
 
 // Allocation-free totals over caller-owned device arrays: validation, the
 // once-per-device scratch lookup, then the two reductions.  Returns codes

@@ -30,6 +30,9 @@ def test_library_exports_every_declared_symbol():
     batch = declared_symbols("quasar_mhd_batch.h")
     assert set(batch) == set(_native.BATCH_EXPORTS)
     assert all(hasattr(lib, s) for s in batch)
+    ind = declared_symbols("quasar_mhd_indicator.h")
+    assert set(ind) == set(_native.INDICATOR_EXPORTS)
+    assert all(hasattr(lib, s) for s in ind)
     ext = declared_symbols("quasar_mhd_ext.h")
     assert set(ext) == set(_native.EXT_EXPORTS)
     assert all(hasattr(lib, s) for s in ext)

@@ -65,3 +65,26 @@ def test_oracle_matches_reference_kernels(oracle, ref):
         w = rng.normal(0, 1, 7)
         assert abs(oracle.mp(w) - ref.mp(w)) <= 1e-13
         assert abs(oracle.mp(w[:5]) - ref.mp(w[:5])) <= 1e-13
+
+
+def test_mlp_oracle_gradient_matches_finite_differences(monkeypatch):
+    """The indicator network's CPU restatement: analytic gradient against
+    central differences (BF16 operand rounding switched off)."""
+    import os
+    import sys
+    import numpy as np
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import mlp_oracle as O
+    monkeypatch.setattr(O, "bf16", lambda a: np.asarray(a, dtype=np.float64))
+    rng = np.random.default_rng(0)
+    p = rng.standard_normal(O.NPARAM) * 0.1
+    X = rng.standard_normal((40, O.FEAT))
+    y = (rng.random(40) < 0.3).astype(float)
+    _, g = O.loss_and_grads(p, X, y, pos_weight=3.0)
+    idx = np.concatenate([rng.integers(0, O.NPARAM, 40), [O.NPARAM - 1]])
+    h = 1e-6
+    for i in idx:
+        e = np.zeros(O.NPARAM)
+        e[i] = h
+        fd = (O.loss_and_grads(p + e, X, y, 3.0)[0] - O.loss_and_grads(p - e, X, y, 3.0)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])
