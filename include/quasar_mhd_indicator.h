@@ -1,7 +1,7 @@
 /*
  * Learned troubled-cell indicator for the MP reconstruction.  No counterpart
- * in the reference; its labels are the reference's own limiter decisions
- * (the negation of the MP early-accept test, numerics/mp_limiter.hpp:84-106).
+ * in the reference; its labels are the reference limiter's own decisions
+ * (numerics/mp_limiter.hpp:71-224) taken in the solver's reconstruction.
  *
  * Network: 200 -> 64 -> 64 -> 1 with GELU, BF16 weights, FP32 accumulation on
  * the tensor cores.  Inputs: the 8 primitives (rho, vx, vy, vz, p, bx, by, bz,
@@ -37,6 +37,51 @@ int qmhd_indicator_set_params(qmhd_indicator* ind, const float* params, size_t n
 /* Logits of `rows` host feature rows (rows x 200 floats, rounded to BF16). */
 int qmhd_indicator_forward(qmhd_indicator* ind, const float* features, long long rows,
                            float* logits);
+
+/* Mean weighted binary cross-entropy of host rows (positives weighted by
+ * pos_weight) and its gradient (QMHD_INDICATOR_PARAMS floats, parameter
+ * packing), from the tensor-core backward pass; no parameter update. */
+int qmhd_indicator_gradient(qmhd_indicator* ind, const float* features,
+                            const unsigned char* labels, long long rows, float pos_weight,
+                            float* grad, size_t n, double* loss);
+
+/* Append every interior cell of the solver's live state to the training set:
+ * its feature row and its label, 1 when a face state whose stencil is
+ * centred on the cell, as the solver's own MP reconstruction (mp5/mp7)
+ * limits it in characteristic fields, departs from the unlimited
+ * component-wise interpolation by more than `tol` of the state's scale
+ * (largest relative difference over rho, momentum against sqrt(2 rho E),
+ * energy, field against sqrt(2 E)).  Where no face departs more than tol the
+ * learned step's fast path reproduces the plain step within tol.  (The
+ * early-accept test of numerics/mp_limiter.hpp:84-106 alone fails in nearly
+ * every cell: near-constant fields fail it by sign noise while the limiter
+ * moves them by rounding only.) */
+int qmhd_indicator_collect(qmhd_indicator* ind, qmhd_solver* solver, float tol);
+long long qmhd_indicator_rows(const qmhd_indicator* ind);
+int qmhd_indicator_clear(qmhd_indicator* ind);
+
+/* Adam (beta 0.9 / 0.999) over random 128-row tiles, `tiles_per_step` tiles
+ * per step; one tile in `holdout`, chosen by a hash of the tile index, is held
+ * out (0 = none).  *loss = mean
+ * training loss of the last epoch. */
+int qmhd_indicator_train(qmhd_indicator* ind, int epochs, int tiles_per_step, float lr,
+                         float pos_weight, int holdout, unsigned long long seed, double* loss);
+/* Recall of limiter firings and fraction of rows flagged (logit > threshold)
+ * on the held-out tiles. */
+int qmhd_indicator_evaluate(qmhd_indicator* ind, float threshold, int holdout, double* recall,
+                            double* flagged, long long* positives, long long* total);
+int qmhd_indicator_threshold_for_recall(qmhd_indicator* ind, double recall, int holdout,
+                                        float* threshold);
+
+/* Learned mode of a solver (mp5 / mp7): once per step the indicator scores
+ * the live state; faces next to a cell scored above `threshold` (or without
+ * a full stencil) keep the characteristic MP reconstruction in every stage,
+ * all other faces take the unlimited component-wise interpolation, which
+ * equals the characteristic result wherever the limiter would not fire.
+ * ind = NULL restores the plain step.  The indicator must outlive this use. */
+int qmhd_solver_set_indicator(qmhd_solver* solver, const qmhd_indicator* ind, float threshold);
+/* Faces on the full-reconstruction lists of the last learned step. */
+int qmhd_solver_learned_face_counts(qmhd_solver* solver, long long* x_faces, long long* y_faces);
 
 #ifdef __cplusplus
 }

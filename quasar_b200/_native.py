@@ -30,7 +30,11 @@ BATCH_EXPORTS = ("qmhd_batch_create", "qmhd_batch_destroy", "qmhd_batch_size", "
                  "qmhd_batch_instance", "qmhd_batch_advance", "qmhd_batch_time_steps",
                  "qmhd_batch_autotune", "qmhd_batch_set_tuning")
 INDICATOR_EXPORTS = ("qmhd_indicator_create", "qmhd_indicator_destroy", "qmhd_indicator_get_params",
-                     "qmhd_indicator_set_params", "qmhd_indicator_forward")
+                     "qmhd_indicator_set_params", "qmhd_indicator_forward",
+                     "qmhd_indicator_gradient", "qmhd_indicator_collect", "qmhd_indicator_rows",
+                     "qmhd_indicator_clear", "qmhd_indicator_train", "qmhd_indicator_evaluate",
+                     "qmhd_indicator_threshold_for_recall", "qmhd_solver_set_indicator",
+                     "qmhd_solver_learned_face_counts")
 
 
 class QmhdConfig(ctypes.Structure):
@@ -97,6 +101,20 @@ def lib() -> ctypes.CDLL:
     L.qmhd_indicator_get_params.argtypes = [vp, vp, ctypes.c_size_t]
     L.qmhd_indicator_set_params.argtypes = [vp, vp, ctypes.c_size_t]
     L.qmhd_indicator_forward.argtypes = [vp, vp, ctypes.c_longlong, vp]
+    lp = ctypes.POINTER(ctypes.c_longlong)
+    L.qmhd_indicator_gradient.argtypes = [vp, vp, vp, ctypes.c_longlong, ctypes.c_float, vp,
+                                          ctypes.c_size_t, dp]
+    L.qmhd_indicator_collect.argtypes = [vp, vp, ctypes.c_float]
+    L.qmhd_indicator_rows.argtypes = [vp]
+    L.qmhd_indicator_rows.restype = ctypes.c_longlong
+    L.qmhd_indicator_clear.argtypes = [vp]
+    L.qmhd_indicator_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                       ctypes.c_float, ctypes.c_int, ctypes.c_ulonglong, dp]
+    L.qmhd_indicator_evaluate.argtypes = [vp, ctypes.c_float, ctypes.c_int, dp, dp, lp, lp]
+    L.qmhd_indicator_threshold_for_recall.argtypes = [vp, ctypes.c_double, ctypes.c_int,
+                                                      ctypes.POINTER(ctypes.c_float)]
+    L.qmhd_solver_set_indicator.argtypes = [vp, vp, ctypes.c_float]
+    L.qmhd_solver_learned_face_counts.argtypes = [vp, lp, lp]
     _lib = L
     return L
 

@@ -347,6 +347,89 @@ int qmhd_indicator_forward(qmhd_indicator* ind, const float* features, long long
   });
 }
 
+int qmhd_indicator_gradient(qmhd_indicator* ind, const float* features,
+                            const unsigned char* labels, long long rows, float pos_weight,
+                            float* grad, size_t n, double* loss) {
+  return guarded([&] {
+    need(ind);
+    need(features);
+    need(labels);
+    need(grad);
+    if (n != size_t(QMHD_INDICATOR_PARAMS))
+      throw std::invalid_argument("qmhd_indicator_gradient: need QMHD_INDICATOR_PARAMS floats");
+    const double l = ind->impl.gradient(features, labels, rows, pos_weight, grad);
+    if (loss) *loss = l;
+  });
+}
+
+int qmhd_indicator_collect(qmhd_indicator* ind, qmhd_solver* solver, float tol) {
+  return guarded([&] {
+    need(ind);
+    need(solver);
+    ind->impl.collect(solver->impl->live_args(), solver->impl->stream(), tol);
+  });
+}
+
+long long qmhd_indicator_rows(const qmhd_indicator* ind) { return ind ? ind->impl.rows() : -1; }
+
+int qmhd_indicator_clear(qmhd_indicator* ind) {
+  return guarded([&] {
+    need(ind);
+    ind->impl.clear_rows();
+  });
+}
+
+int qmhd_indicator_train(qmhd_indicator* ind, int epochs, int tiles_per_step, float lr,
+                         float pos_weight, int holdout, unsigned long long seed, double* loss) {
+  return guarded([&] {
+    need(ind);
+    if (epochs < 0 || tiles_per_step < 1 || !(lr > 0.f))
+      throw std::invalid_argument("qmhd_indicator_train: need epochs >= 0, tiles >= 1, lr > 0");
+    const double l = ind->impl.train(epochs, tiles_per_step, lr, pos_weight, holdout, seed);
+    if (loss) *loss = l;
+  });
+}
+
+int qmhd_indicator_evaluate(qmhd_indicator* ind, float threshold, int holdout, double* recall,
+                            double* flagged, long long* positives, long long* total) {
+  return guarded([&] {
+    need(ind);
+    double r = 0, f = 0;
+    long long p = 0, t = 0;
+    ind->impl.evaluate(threshold, holdout, &r, &f, &p, &t);
+    if (recall) *recall = r;
+    if (flagged) *flagged = f;
+    if (positives) *positives = p;
+    if (total) *total = t;
+  });
+}
+
+int qmhd_indicator_threshold_for_recall(qmhd_indicator* ind, double recall, int holdout,
+                                        float* threshold) {
+  return guarded([&] {
+    need(ind);
+    need(threshold);
+    *threshold = ind->impl.threshold_for_recall(recall, holdout);
+  });
+}
+
+int qmhd_solver_set_indicator(qmhd_solver* solver, const qmhd_indicator* ind, float threshold) {
+  return guarded([&] {
+    need(solver);
+    solver->impl->set_indicator(ind ? &ind->impl : nullptr, threshold);
+  });
+}
+
+int qmhd_solver_learned_face_counts(qmhd_solver* solver, long long* x_faces, long long* y_faces) {
+  return guarded([&] {
+    need(solver);
+    long long a = 0, b = 0;
+    solver->impl->learned_face_counts(&a, &b);
+    if (x_faces) *x_faces = a;
+    if (y_faces) *y_faces = b;
+  });
+}
+
 // Allocation-free totals over caller-owned device arrays: validation, the
 // once-per-device scratch lookup, then the two reductions.  Returns codes
 // directly (no exceptions) so the success path allocates nothing on the host.

@@ -277,27 +277,39 @@ __device__ __forceinline__ double mp_limit(double vl, double vm2, double vm1, do
 }
 // mp_limiter.hpp:182-224: W = 5 (MP5) or 7 (MP7); v[0..W-1].  The stencil is
 // normalised by its largest magnitude through one reciprocal.
+// Unlimited MP interpolation of the W-point stencil v[] to the face:
+// normalised by the stencil's largest magnitude through one reciprocal.
 template <int W>
-__device__ __forceinline__ double mp_recon(const double* v, bool& fired) {
+__device__ __forceinline__ double mp_interp(const double* v) {
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < W; ++k) s = fmax(s, fabs(v[k]));
-  double vl;
-  if (s == 0.0) {
-    vl = 0.0;
-  } else {
-    const double is = 1.0 / s;
-    if (W == 5) {
-      const double sum = 2.0 * (v[0] * is) - 13.0 * (v[1] * is) + 47.0 * (v[2] * is) +
-                         27.0 * (v[3] * is) - 3.0 * (v[4] * is);
-      vl = (sum * (1.0 / 60.0)) * s;
-    } else {
-      const double sum = -3.0 * (v[0] * is) + 25.0 * (v[1] * is) - 101.0 * (v[2] * is) +
-                         319.0 * (v[3] * is) + 214.0 * (v[4] * is) - 38.0 * (v[5] * is) +
-                         4.0 * (v[6] * is);
-      vl = (sum * (1.0 / 420.0)) * s;
-    }
+  if (s == 0.0) return 0.0;
+  const double is = 1.0 / s;
+  if (W == 5) {
+    const double sum = 2.0 * (v[0] * is) - 13.0 * (v[1] * is) + 47.0 * (v[2] * is) +
+                       27.0 * (v[3] * is) - 3.0 * (v[4] * is);
+    return (sum * (1.0 / 60.0)) * s;
   }
+  const double sum = -3.0 * (v[0] * is) + 25.0 * (v[1] * is) - 101.0 * (v[2] * is) +
+                     319.0 * (v[3] * is) + 214.0 * (v[4] * is) - 38.0 * (v[5] * is) +
+                     4.0 * (v[6] * is);
+  return (sum * (1.0 / 420.0)) * s;
+}
+
+// The same interpolation without the magnitude normalisation (the
+// component-wise fast path, where overflow guarding is not needed).
+template <int W>
+__device__ __forceinline__ double mp_interp_plain(const double* v) {
+  if (W == 5)
+    return (2.0 * v[0] - 13.0 * v[1] + 47.0 * v[2] + 27.0 * v[3] - 3.0 * v[4]) * (1.0 / 60.0);
+  return (-3.0 * v[0] + 25.0 * v[1] - 101.0 * v[2] + 319.0 * v[3] + 214.0 * v[4] - 38.0 * v[5] +
+          4.0 * v[6]) * (1.0 / 420.0);
+}
+
+template <int W>
+__device__ __forceinline__ double mp_recon(const double* v, bool& fired) {
+  const double vl = mp_interp<W>(v);
   constexpr int o = W == 5 ? 0 : 1;
   return mp_limit(vl, v[o], v[o + 1], v[o + 2], v[o + 3], v[o + 4], fired);
 }

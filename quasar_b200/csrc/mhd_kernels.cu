@@ -589,6 +589,54 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
   ur = rot<DIR>(sr);
 }
 
+// Component-wise unlimited MP interpolation of the same conserved deltas:
+// the characteristic path with L = R = I and no limiter, which equals the
+// characteristic result wherever the limiter accepts every wave (R L = I).
+template <int DIR, int H>
+__device__ void mp_pair_lin(const StateP& u, long long k0, long long step, St& ul, St& ur) {
+  constexpr int S = 2 * H + 2, W = 2 * H + 1;
+  const St cl = load_cell(u, k0 - step), cr = load_cell(u, k0);
+  St ref;
+  ref.rho = 0.5 * cl.rho + 0.5 * cr.rho;
+  ref.mx = 0.5 * cl.mx + 0.5 * cr.mx;
+  ref.my = 0.5 * cl.my + 0.5 * cr.my;
+  ref.mz = 0.5 * cl.mz + 0.5 * cr.mz;
+  ref.E = 0.5 * cl.E + 0.5 * cr.E;
+  ref.bx = 0.5 * cl.bx + 0.5 * cr.bx;
+  ref.by = 0.5 * cl.by + 0.5 * cr.by;
+  ref.bz = 0.5 * cl.bz + 0.5 * cr.bz;
+  const St c = rot<DIR>(ref);
+  double u7[S][7];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const St d = rot<DIR>(load_cell(u, k0 + (long long)(s - 1 - H) * step));
+    u7[s][0] = d.rho - c.rho;
+    u7[s][1] = d.mx - c.mx;
+    u7[s][2] = d.my - c.my;
+    u7[s][3] = d.mz - c.mz;
+    u7[s][4] = d.E - c.E;
+    u7[s][5] = d.by - c.by;
+    u7[s][6] = d.bz - c.bz;
+  }
+  double dl[7], dr[7];
+#pragma unroll
+  for (int v = 0; v < 7; ++v) {
+    double win[W];
+#pragma unroll
+    for (int s = 0; s < W; ++s) win[s] = u7[s][v];
+    dl[v] = mp_interp_plain<W>(win);
+#pragma unroll
+    for (int s = 0; s < W; ++s) win[s] = u7[W - s][v];
+    dr[v] = mp_interp_plain<W>(win);
+  }
+  const St sl{c.rho + dl[0], c.mx + dl[1], c.my + dl[2], c.mz + dl[3],
+              c.E + dl[4],   c.bx,         c.by + dl[5], c.bz + dl[6]};
+  const St sr{c.rho + dr[0], c.mx + dr[1], c.my + dr[2], c.mz + dr[3],
+              c.E + dr[4],   c.bx,         c.by + dr[5], c.bz + dr[6]};
+  ul = rot<DIR>(sl);
+  ur = rot<DIR>(sr);
+}
+
 // ---- MUSCL-minmod in primitive variables (mhd_reconstruct.hip:93-404) ----
 __device__ __forceinline__ int slope_drop(int c, int n, int lo, int hi) {
   if (lo != 0 && lo != 4 && c <= 0) return -1;
@@ -628,14 +676,32 @@ __device__ void muscl_pair(const Grid& g, const StateP& u, int i, int j, long lo
   ur = to_cons(muscl_face(b, c, d, -1.0, slope_drop(pos, n, lo, hi)), gamma);
 }
 
-template <int DIR, int ORDER>
-__device__ __forceinline__ void b_reconstruct(const Grid& g, const StateP& u, const IfaceP& out,
-                                              double gamma, const Ctl* ctl, int bx, int by) {
-  // dir 0: faces i in [0,nx] over all padded rows; dir 1: transposed.
-  const int i = bx * blockDim.x + threadIdx.x - (DIR == 1 ? g.ng : 0);
-  const int j = by * blockDim.y + threadIdx.y - (DIR == 0 ? g.ng : 0);
-  if (DIR == 0 ? (i > g.nx || j >= g.ny + g.ng) : (i >= g.nx + g.ng || j > g.ny)) return;
-  if (ctl->status & ~kStatusDone) return;
+// How far the limited characteristic face state departs from the unlimited
+// component-wise one: the largest difference relative to the state's scale
+// per group (rho; momentum against sqrt(2 rho E); E; field against
+// sqrt(2 E)); +inf when not finite.
+__device__ __forceinline__ float limiter_departure(const St& a, const St& b) {
+  const double rs = fabs(b.rho), es = fabs(b.E);
+  const double ms = sqrt(2.0 * rs * es), bs = sqrt(2.0 * es);
+  double d = fabs(a.rho - b.rho) / rs;
+  d = fmax(d, fabs(a.mx - b.mx) / ms);
+  d = fmax(d, fabs(a.my - b.my) / ms);
+  d = fmax(d, fabs(a.mz - b.mz) / ms);
+  d = fmax(d, fabs(a.E - b.E) / es);
+  d = fmax(d, fabs(a.bx - b.bx) / bs);
+  d = fmax(d, fabs(a.by - b.by) / bs);
+  d = fmax(d, fabs(a.bz - b.bz) / bs);
+  return isfinite(d) ? float(d) : INFINITY;
+}
+
+// One face's interface states.  MODE 0: the characteristic MP path; 1: the
+// same, also recording per cell the largest departure of a limited state
+// from the unlimited component-wise one (label[cell] = max, as float bits;
+// the left state's stencil is centred on the left cell);
+// 2: the unlimited component-wise path.  Orders 1 and 2 ignore MODE.
+template <int DIR, int ORDER, int MODE>
+__device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const IfaceP& out,
+                                           double gamma, int i, int j, int* label) {
   const long long k0 = g.idx(i, j);
   const long long step = DIR == 0 ? 1 : g.pitch;
   St ul, ur;
@@ -645,7 +711,19 @@ __device__ __forceinline__ void b_reconstruct(const Grid& g, const StateP& u, co
   } else if (ORDER == 2) {
     muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
   } else {
-    mp_pair_loop<DIR, ORDER == 5 ? 2 : 3>(u, k0, step, gamma, ul, ur);
+    constexpr int H = ORDER == 5 ? 2 : 3;
+    if (MODE == 2) {
+      mp_pair_lin<DIR, H>(u, k0, step, ul, ur);
+    } else {
+      mp_pair_loop<DIR, H>(u, k0, step, gamma, ul, ur);
+      if (MODE == 1) {
+        St ll, lr;
+        mp_pair_lin<DIR, H>(u, k0, step, ll, lr);
+        // non-negative floats order like their bit patterns
+        atomicMax(label + (k0 - step), __float_as_int(limiter_departure(ul, ll)));
+        atomicMax(label + k0, __float_as_int(limiter_departure(ur, lr)));
+      }
+    }
     if (!recon_admissible(ul, gamma) || !recon_admissible(ur, gamma))
       muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
   }
@@ -675,10 +753,80 @@ __device__ __forceinline__ void b_reconstruct(const Grid& g, const StateP& u, co
   }
 }
 
+template <int DIR, int ORDER, int MODE = 0>
+__device__ __forceinline__ void b_reconstruct(const Grid& g, const StateP& u, const IfaceP& out,
+                                              double gamma, const Ctl* ctl, int bx, int by,
+                                              int* label = nullptr) {
+  // dir 0: faces i in [0,nx] over all padded rows; dir 1: transposed.
+  const int i = bx * blockDim.x + threadIdx.x - (DIR == 1 ? g.ng : 0);
+  const int j = by * blockDim.y + threadIdx.y - (DIR == 0 ? g.ng : 0);
+  if (DIR == 0 ? (i > g.nx || j >= g.ny + g.ng) : (i >= g.nx + g.ng || j > g.ny)) return;
+  if (ctl->status & ~kStatusDone) return;
+  recon_face<DIR, ORDER, MODE>(g, u, out, gamma, i, j, label);
+}
+
 template <int DIR, int ORDER>
 __global__ void __launch_bounds__(128) k_reconstruct(Grid g, StateP u, IfaceP out, double gamma,
                                                      const Ctl* ctl) {
   b_reconstruct<DIR, ORDER>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y);
+}
+
+// Limiter labels of the cells (training data of the indicator).
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128) k_reconstruct_label(Grid g, StateP u, IfaceP out,
+                                                           double gamma, const Ctl* ctl,
+                                                           int* label) {
+  b_reconstruct<DIR, ORDER, 1>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y, label);
+}
+
+// Learned mode, pass 1: every face by the unlimited component-wise path.
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128) k_reconstruct_lin(Grid g, StateP u, IfaceP out,
+                                                         double gamma, const Ctl* ctl) {
+  b_reconstruct<DIR, ORDER, 2>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y);
+}
+
+// Learned mode, pass 2: the listed faces (padded linear index of the face's
+// high cell) by the full characteristic path; the count is read on the device.
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128) k_reconstruct_list(Grid g, StateP u, IfaceP out,
+                                                          double gamma, const Ctl* ctl,
+                                                          const int* list, const int* count) {
+  if (ctl->status & ~kStatusDone) return;
+  const int n = *count;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int k = list[t];
+    const int i = k % g.pitch - g.ng, j = k / g.pitch - g.ng;
+    recon_face<DIR, ORDER, 0>(g, u, out, gamma, i, j, nullptr);
+  }
+}
+
+// Faces whose either cell is flagged, appended to the x and y lists in
+// warp-aggregated order; padded cells are scanned row-major.
+__global__ void k_face_lists(Grid g, const unsigned char* flag, int* xlist, int* ylist,
+                             int* counts) {
+  const long long n = g.size();
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31;
+  bool nx_ = false, ny_ = false;
+  int k = 0;
+  if (t < n) {
+    k = int(t);
+    const int i = int(t % g.pitch) - g.ng, j = int(t / g.pitch) - g.ng;
+    if (i >= 0 && i <= g.nx && j < g.ny + g.ng) nx_ = (flag[t] | flag[t - 1]) != 0;
+    if (j >= 0 && j <= g.ny && i < g.nx + g.ng) ny_ = (flag[t] | flag[t - g.pitch]) != 0;
+  }
+  const unsigned bx_ = __ballot_sync(0xffffffffu, nx_), by_ = __ballot_sync(0xffffffffu, ny_);
+  int basex = 0, basey = 0;
+  if (lane == 0) {
+    if (bx_) basex = atomicAdd(&counts[0], __popc(bx_));
+    if (by_) basey = atomicAdd(&counts[1], __popc(by_));
+  }
+  basex = __shfl_sync(0xffffffffu, basex, 0);
+  basey = __shfl_sync(0xffffffffu, basey, 0);
+  const unsigned below = (1u << lane) - 1u;
+  if (nx_) xlist[basex + __popc(bx_ & below)] = k;
+  if (ny_) ylist[basey + __popc(by_ & below)] = k;
 }
 
 
@@ -1916,6 +2064,49 @@ void launch_batch_colloc_check(const BatchRec* r, const BatchPlan& p, int order,
 
 void launch_batch_ctl(const BatchRec* r, int n, int what, double t, double t_end, cudaStream_t s) {
   kb_ctl<<<cdiv(n, 128), 128, 0, s>>>(r, n, what, t, t_end);
+}
+
+// ---- learned-mode reconstruction and indicator training data ----------------
+namespace {
+template <int DIR, int ORDER>
+dim3 recon_grid(const Grid& g) {
+  const int ni = DIR == 0 ? g.nx + 1 : g.nx + 2 * g.ng;
+  const int nj = DIR == 0 ? g.ny + 2 * g.ng : g.ny + 1;
+  return dim3(cdiv(ni, kBX), cdiv(nj, 4));
+}
+}  // namespace
+
+void launch_reconstruct_label(const StageArgs& a, int dir, int* label, cudaStream_t s) {
+  const dim3 block(kBX, 4);
+  const IfaceP out = dir == 0 ? a.ix : a.iy;
+#define QB_LBL(D, O)                                                                          \
+  if (dir == D && a.order == O)                                                              \
+    return (void)k_reconstruct_label<D, O><<<recon_grid<D, O>(a.g), block, 0, s>>>(         \
+        a.g, a.u, out, a.gamma, a.ctl, label);
+  QB_LBL(0, 5) QB_LBL(1, 5) QB_LBL(0, 7) QB_LBL(1, 7)
+#undef QB_LBL
+}
+
+void launch_reconstruct_learned(const StageArgs& a, int dir, const int* list, const int* count,
+                                int list_grid, cudaStream_t s) {
+  const dim3 block(kBX, 4);
+  const IfaceP out = dir == 0 ? a.ix : a.iy;
+#define QB_LRN(D, O)                                                                          \
+  if (dir == D && a.order == O) {                                                            \
+    k_reconstruct_lin<D, O><<<recon_grid<D, O>(a.g), block, 0, s>>>(a.g, a.u, out, a.gamma,  \
+                                                                    a.ctl);                  \
+    k_reconstruct_list<D, O><<<list_grid, 128, 0, s>>>(a.g, a.u, out, a.gamma, a.ctl, list,   \
+                                                       count);                               \
+    return;                                                                                  \
+  }
+  QB_LRN(0, 5) QB_LRN(1, 5) QB_LRN(0, 7) QB_LRN(1, 7)
+#undef QB_LRN
+}
+
+void launch_face_lists(const Grid& g, const unsigned char* flag, int* xlist, int* ylist,
+                       int* counts, cudaStream_t s) {
+  cudaMemsetAsync(counts, 0, 2 * sizeof(int), s);
+  k_face_lists<<<cdiv(g.size(), 256), 256, 0, s>>>(g, flag, xlist, ylist, counts);
 }
 
 }  // namespace qb

@@ -175,4 +175,19 @@ void launch_batch_colloc_check(const BatchRec* r, const BatchPlan& p, int order,
 // 2 step_end, 3 set_time(t, t_end).
 void launch_batch_ctl(const BatchRec* r, int n, int what, double t, double t_end, cudaStream_t s);
 
+// ---- learned troubled-cell mode --------------------------------------------
+// Limiter departures (per padded cell, float bits, max-reduced): how far a
+// face state of a stencil centred on the cell, limited in characteristic
+// fields, departs from the unlimited component-wise state, relative to the
+// state's scale.  The array must start at zero.
+void launch_reconstruct_label(const StageArgs& a, int dir, int* label, cudaStream_t s);
+// Unlimited component-wise reconstruction of every face, then the full
+// characteristic path for the listed faces (count on the device).
+void launch_reconstruct_learned(const StageArgs& a, int dir, const int* list, const int* count,
+                                int list_grid, cudaStream_t s);
+// Faces adjacent to a flagged cell (flag per padded cell) -> x / y lists;
+// counts[0..1] are reset first.
+void launch_face_lists(const Grid& g, const unsigned char* flag, int* xlist, int* ylist,
+                       int* counts, cudaStream_t s);
+
 }  // namespace qb

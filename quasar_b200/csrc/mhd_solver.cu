@@ -3,6 +3,7 @@
 // MhdSolver2D (src/physics/mhd/mhd_solver.cpp) call for call where the
 // semantics are observable: preflights, CFL cap, retry policy, errors.
 #include "mhd_solver.cuh"
+#include "indicator.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -106,6 +107,10 @@ MhdSolver2D::~MhdSolver2D() {
   for (auto& ge : graph_)
     if (ge) cudaGraphExecDestroy(ge);
   cudaStreamSynchronize(stream_);
+  cudaFree(flags_);
+  cudaFree(flists_);
+  cudaFree(fcounts_);
+  cudaFree(ind_status_);
   cudaFree(arena_);
   cudaFree(iarena_);
   cudaFree(ctl_);
@@ -205,8 +210,15 @@ void MhdSolver2D::front_impl(int order, int dt_mode, int anchor_mode) {
   launch_step_begin(ctl_, order <= 1 ? 1 : 0, anchor_mode, stream_);
   mark(0);
   const StageArgs a = stage_args(st_[live_], order);
-  launch_reconstruct(a, 0, stream_);
-  launch_reconstruct(a, 1, stream_);
+  if (ind_ && order >= 5) {
+    // score the live state once per step; unwritten flags stay 1 (full path)
+    ck(cudaMemsetAsync(flags_, 1, size_t(g_.size()), stream_), "flags");
+    ck(launch_indicator(g_, st_[live_], cfg_.gamma, ind_->dev(), ind_threshold_, flags_,
+                        ind_status_, stream_),
+       "indicator launch");
+    launch_face_lists(g_, flags_, flists_, flists_ + g_.size(), fcounts_, stream_);
+  }
+  reconstruct_stage(a, order);
   mark(1);
   const bool speeds = dt_mode != 0;
   launch_face_flux(a, 0, speeds, stream_);
@@ -222,6 +234,63 @@ void MhdSolver2D::front_impl(int order, int dt_mode, int anchor_mode) {
               stream_);
     mark(0);
   }
+}
+
+void MhdSolver2D::reconstruct_stage(const StageArgs& a, int order) {
+  if (ind_ && order >= 5) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    launch_reconstruct_learned(a, 0, flists_, fcounts_, 2 * sms, stream_);
+    launch_reconstruct_learned(a, 1, flists_ + g_.size(), fcounts_ + 1, 2 * sms, stream_);
+  } else {
+    launch_reconstruct(a, 0, stream_);
+    launch_reconstruct(a, 1, stream_);
+  }
+}
+
+StageArgs MhdSolver2D::live_args() {
+  ensure_live_ready();
+  return stage_args(st_[live_], cfg_.order);
+}
+
+void MhdSolver2D::release_graphs() {
+  for (auto& ge : graph_) {
+    if (ge) cudaGraphExecDestroy(ge);
+    ge = nullptr;
+  }
+}
+
+void MhdSolver2D::set_indicator(const Indicator* ind, float threshold) {
+  if (ind && cfg_.order != 5 && cfg_.order != 7)
+    throw std::invalid_argument("MhdSolver2D: the learned indicator needs mp5 or mp7");
+  if (ind && !std::isfinite(threshold))
+    throw std::invalid_argument("MhdSolver2D: indicator threshold must be finite");
+  if (ind) ck(configure_indicator_kernels(), "indicator kernels");
+  if (ind && !flags_) {
+    ck(cudaMalloc(&flags_, size_t(g_.size())), "indicator flags");
+    ck(cudaMalloc(&flists_, sizeof(int) * 2 * size_t(g_.size())), "face lists");
+    ck(cudaMalloc(&fcounts_, sizeof(int) * 2), "face counts");
+    ck(cudaMalloc(&ind_status_, sizeof(int)), "indicator status");
+    ck(cudaMemsetAsync(fcounts_, 0, sizeof(int) * 2, stream_), "face counts");
+    ck(cudaMemsetAsync(ind_status_, 0, sizeof(int), stream_), "indicator status");
+  }
+  ind_ = ind;
+  ind_threshold_ = threshold;
+  front_order_ = 0;
+  release_graphs();
+}
+
+void MhdSolver2D::learned_face_counts(long long* nxf, long long* nyf) {
+  int c[2] = {0, 0}, st = 0;
+  if (fcounts_) {
+    ck(cudaMemcpyAsync(c, fcounts_, sizeof c, cudaMemcpyDeviceToHost, stream_), "face counts");
+    ck(cudaMemcpyAsync(&st, ind_status_, sizeof st, cudaMemcpyDeviceToHost, stream_), "status");
+    ck(cudaStreamSynchronize(stream_), "face counts");
+  }
+  if (st) throw std::runtime_error("MhdSolver2D: indicator tensor-core wait ran out");
+  *nxf = c[0];
+  *nyf = c[1];
 }
 
 // Stages of one SSP-RK3 step after the cached stage-0 residual
@@ -241,8 +310,7 @@ void MhdSolver2D::finish_impl(int order, const double* dt_dev, double dt_host, b
     const StateP in = stage == 1 ? u1 : u2;
     const StateP out = stage == 1 ? u2 : nxt;
     const StageArgs a = stage_args(in, order);
-    launch_reconstruct(a, 0, stream_);
-    launch_reconstruct(a, 1, stream_);
+    reconstruct_stage(a, order);
     mark(1);
     launch_face_flux(a, 0, false, stream_);
     launch_face_flux(a, 1, false, stream_);

@@ -32,6 +32,7 @@ struct CudaError : std::runtime_error {
 };
 
 class MhdBatch2D;
+class Indicator;
 
 class MhdSolver2D {
  public:
@@ -71,6 +72,18 @@ class MhdSolver2D {
 
   // Device pointers of the live state (kernel-level C-ABI and tests).
   double* live_component(int comp) const;
+  // Stage arguments of the live state after its preflight (ghosts filled,
+  // field collocated), for kernels run on the solver's state from outside.
+  StageArgs live_args();
+
+  // Learned troubled-cell mode (mp5/mp7): once per step the indicator scores
+  // the live state's cells; faces next to a cell scored above `threshold`
+  // keep the characteristic MP reconstruction in every stage, all others
+  // take the unlimited component-wise interpolation.  nullptr turns it off.
+  // The indicator must outlive its use by this solver.
+  void set_indicator(const Indicator* ind, float threshold);
+  // Faces on the full-reconstruction lists of the last step, x and y.
+  void learned_face_counts(long long* nx_faces, long long* ny_faces);
   cudaStream_t stream() const { return stream_; }
 
  private:
@@ -118,6 +131,15 @@ class MhdSolver2D {
   int low_order_ = 0;           // 1 while the positivity controller runs low order
   int last_substeps_ = 0;
   cudaGraphExec_t graph_[2] = {nullptr, nullptr};
+  void release_graphs();
+  void reconstruct_stage(const StageArgs& a, int order);
+  // learned mode
+  const Indicator* ind_ = nullptr;
+  float ind_threshold_ = 0.f;
+  unsigned char* flags_ = nullptr;   // per padded cell
+  int* flists_ = nullptr;            // x list, y list (padded size each)
+  int* fcounts_ = nullptr;           // [2]
+  int* ind_status_ = nullptr;
   // per-phase event marks while profiling (phase, event after the launch)
   struct Mark {
     int phase;

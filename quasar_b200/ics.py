@@ -47,33 +47,34 @@ def orszag_tang(n, order=5, gamma=5.0 / 3.0, amplitude=1.0, ny=None):
                      -b0 * np.sin(2 * pi * Y), b0 * np.sin(4 * pi * X), z, gamma)
 
 
-def rotor(n, order=7, gamma=5.0 / 3.0, ny=None):
-    """rho=10 for r<0.1, linear taper to 1 at r=0.115, rigid rotation u0=2 at
-    r0=0.1 tapering to rest at r1, p=1, Bx=5/sqrt(4 pi) (mhd_initial_conditions.hip:159-188)."""
+def rotor(n, order=7, gamma=5.0 / 3.0, ny=None, r0=0.1, bx=5.0 / math.sqrt(4.0 * math.pi)):
+    """rho=10 for r<r0, linear taper to 1 at r1 = 1.15 r0, rigid rotation
+    u0=2 at r0 tapering to rest at r1, p=1, Bx=5/sqrt(4 pi)
+    (mhd_initial_conditions.hip:159-188)."""
     ng = nghost(order)
     ny = n if ny is None else ny
     X, Y = np.meshgrid(_centres(n, ng), _centres(ny, ng), indexing="xy")
     rx, ry = X - 0.5, Y - 0.5
     r = np.hypot(rx, ry)
-    r0, r1, u0 = 0.1, 0.115, 2.0
+    r1, u0 = 1.15 * r0, 2.0
     f = np.clip((r1 - r) / (r1 - r0), 0.0, 1.0)
     f = np.where(r <= r0, 1.0, np.where(r >= r1, 0.0, f))
     with np.errstate(divide="ignore", invalid="ignore"):
         sf = np.where(r <= r0, u0 / r0, np.where(r < r1, f * u0 / np.maximum(r, 1e-300), 0.0))
     z = np.zeros_like(X)
     return _assemble(1.0 + f * 9.0, -sf * ry, sf * rx, z, np.ones_like(X),
-                     np.full_like(X, 5.0 / math.sqrt(4.0 * math.pi)), z, z, gamma)
+                     np.full_like(X, bx), z, z, gamma)
 
 
-def blast(n, order=7, gamma=5.0 / 3.0, ny=None):
+def blast(n, order=7, gamma=5.0 / 3.0, ny=None, radius=0.1, p_in=100.0, p_out=0.1,
+          b=10.0 / math.sqrt(8.0 * math.pi)):
     """p=100 for r<0.1 else 0.1, rho=1, Bx=By=10/sqrt(8 pi) (mhd_initial_conditions.hip:145-157)."""
     ng = nghost(order)
     ny = n if ny is None else ny
     X, Y = np.meshgrid(_centres(n, ng), _centres(ny, ng), indexing="xy")
     r = np.hypot(X - 0.5, Y - 0.5)
-    b = 10.0 / math.sqrt(8.0 * math.pi)
     z = np.zeros_like(X)
-    return _assemble(np.ones_like(X), z, z, z, np.where(r < 0.1, 100.0, 0.1),
+    return _assemble(np.ones_like(X), z, z, z, np.where(r < radius, p_in, p_out),
                      np.full_like(X, b), np.full_like(X, b), z, gamma)
 
 
@@ -294,4 +295,48 @@ def batch_instances(count=256, seed=0, lo=64, hi=512, order=5):
                             ly=ny * OBLIQUE_H, gamma=5.0 / 3.0, bc=0, angle=ang,
                             arrays=lambda nx=nx, ny=ny, ang=ang, kind=kind: linear_wave(
                                 nx, ny, order=order, angle=ang, kind=kind)[0]))
+    return out
+
+
+def training_runs(count=12, seed=1, n=512, order=5):
+    """Seeded plain-method runs for the indicator's training labels: rotor
+    (radius log-uniform in [0.05, 0.2], field log-uniform in [0.1, 10]),
+    blast (radius in [0.05, 0.2], pressure ratio in [10, 1000], field in
+    [0.1, 10]) and Orszag-Tang (field scale in [0.1, 10] as amplitude of B^2
+    relative to the gas), cycled in that order.  Returns dicts with family,
+    parameters, bc and a zero-argument `arrays` callable."""
+    rng = np.random.default_rng(seed)
+    lu = lambda a, b: float(math.exp(rng.uniform(math.log(a), math.log(b))))  # noqa: E731
+    out = []
+    for k in range(count):
+        fam = ("rotor", "blast", "orszag_tang")[k % 3]
+        if fam == "rotor":
+            r0, bf = lu(0.05, 0.2), lu(0.1, 10.0)
+            out.append(dict(family=fam, radius=r0, field=bf, bc=1,
+                            arrays=lambda r0=r0, bf=bf: rotor(n, order=order, r0=r0, bx=bf)))
+        elif fam == "blast":
+            r0, ratio, bf = lu(0.05, 0.2), lu(10.0, 1000.0), lu(0.1, 10.0)
+            out.append(dict(family=fam, radius=r0, ratio=ratio, field=bf, bc=1,
+                            arrays=lambda r0=r0, ratio=ratio, bf=bf: blast(
+                                n, order=order, radius=r0, p_in=0.1 * ratio, p_out=0.1,
+                                b=bf / math.sqrt(2.0))))
+        else:
+            amp = lu(0.1, 10.0)
+            out.append(dict(family=fam, field=amp, bc=0,
+                            arrays=lambda amp=amp: _ot_field_scaled(n, order, amp)))
+    return out
+
+
+def _ot_field_scaled(n, order, scale):
+    """Orszag-Tang with the magnetic field scaled by sqrt(scale) at fixed gas
+    state (plasma beta divided by `scale`)."""
+    arr = orszag_tang(n, order=order)
+    ng = nghost(order)
+    out = list(arr)
+    f = math.sqrt(scale)
+    bx, by = arr[5] * f, arr[6] * f
+    # energy: gas + kinetic unchanged, magnetic energy of the scaled field
+    old_mag = 0.5 * (arr[5] ** 2 + arr[6] ** 2)
+    out[4] = np.ascontiguousarray(arr[4] - old_mag + 0.5 * (bx ** 2 + by ** 2))
+    out[5], out[6] = np.ascontiguousarray(bx), np.ascontiguousarray(by)
     return out

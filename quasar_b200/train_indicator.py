@@ -1,0 +1,99 @@
+"""Train the troubled-cell indicator on the GPU and write its parameters.
+
+    python -m quasar_b200.train_indicator --out quasar_b200/data/indicator_mp5.npz
+
+Labels come from plain-method runs of the seeded rotor / blast / Orszag-Tang
+families of `quasar_b200.ics.training_runs`: every `every` steps the live
+state of each run is collected (features of every interior cell and whether
+its limited characteristic face states depart from the component-wise
+unlimited ones), then Adam trains the network with the tensor-core
+forward/backward kernels.  The threshold is the smallest logit that keeps
+`recall` of the held-out limiter activations.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import ics, mhd
+from .indicator import TroubledCellIndicator
+
+
+def _solver(n, order, bc):
+    cfg = mhd.MhdConfig()
+    cfg.grid = mhd.Grid2D(n, n, 1.0, 1.0)
+    cfg.reconstruction = "mp5" if order == 5 else "mp7"
+    side = "periodic" if bc == 0 else "outflow"
+    cfg.boundary = mhd.MhdBoundarySpec([side] * 4, [side] * 4)
+    return mhd.MhdSolver2D(cfg)
+
+
+def collect(ind, n=512, runs=12, steps=400, every=20, order=5, seed=1, tol=1e-6, log=print):
+    t0 = time.time()
+    for k, run in enumerate(ics.training_runs(count=runs, seed=seed, n=n, order=order)):
+        s = _solver(n, order, run["bc"])
+        for name, a in zip(ics.COMPONENTS, run["arrays"]()):
+            s.seed_state(name, a)
+        t, done = 0.0, 0
+        while done < steps:
+            try:
+                t, taken = s.advance_auto(t, 1e30, every)
+            except RuntimeError as e:  # a run the plain method cannot continue ends here
+                log(f"run {k} ({run['family']}) stops after {done} steps: {e}")
+                break
+            done += taken
+            ind.collect(s, tol)
+        log(f"run {k} {run['family']}: {done} steps, rows {ind.rows()} ({time.time() - t0:.0f}s)")
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "data", "indicator_mp5.npz"))
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--runs", type=int, default=12)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--every", type=int, default=20)
+    ap.add_argument("--order", type=int, default=5)
+    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--tiles", type=int, default=512)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--pos-weight", type=float, default=8.0)
+    ap.add_argument("--recall", type=float, default=0.995)
+    ap.add_argument("--holdout", type=int, default=20)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    a = ap.parse_args(argv)
+    ind = TroubledCellIndicator(seed=a.seed)
+    collect(ind, a.n, a.runs, a.steps, a.every, a.order, a.seed, a.tol)
+    t0 = time.time()
+    losses = []
+    for ep in range(a.epochs):
+        lr = a.lr * (0.5 ** (ep // max(1, a.epochs // 3)))
+        losses.append(ind.train(epochs=1, tiles_per_step=a.tiles, lr=lr, pos_weight=a.pos_weight,
+                                holdout=a.holdout, seed=a.seed + ep))
+        print(f"epoch {ep + 1}: loss {losses[-1]:.5f} lr {lr:.2e} ({time.time() - t0:.1f}s)")
+    thr = ind.threshold_for_recall(a.recall, a.holdout)
+    ev = ind.evaluate(thr, a.holdout)
+    print(f"threshold {thr:.4f}: held-out recall {ev['recall']:.4f}, flagged {ev['flagged']:.4f}, "
+          f"positives {ev['positives']} of {ev['total']}")
+    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+    meta = dict(vars(a), rows=ind.rows(), losses=losses, threshold=thr, **ev)
+    np.savez(a.out, params=ind.params(), threshold=np.float32(thr), meta=json.dumps(meta))
+    return ind, thr, ev
+
+
+def load(path=None):
+    """(indicator, threshold) from a file written by main()."""
+    path = path or os.path.join(os.path.dirname(__file__), "data", "indicator_mp5.npz")
+    z = np.load(path)
+    ind = TroubledCellIndicator(seed=0)
+    ind.set_params(z["params"])
+    return ind, float(z["threshold"])
+
+
+if __name__ == "__main__":
+    main()

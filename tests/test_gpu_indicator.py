@@ -30,3 +30,92 @@ def test_forward_matches_oracle(rows):
     want, _ = O.forward(p, x)
     scale = np.max(np.abs(want)) + 1e-30
     assert np.max(np.abs(got - want)) <= 2e-3 * scale, np.max(np.abs(got - want)) / scale
+
+
+def test_gradient_matches_oracle():
+    from quasar_b200.indicator import TroubledCellIndicator
+    ind = TroubledCellIndicator(seed=5)
+    p = ind.params()
+    rng = np.random.default_rng(6)
+    p += (rng.standard_normal(p.shape) * 0.02).astype(np.float32)
+    ind.set_params(p)
+    x = random_rows(1000, 7)
+    y = (rng.random(1000) < 0.3).astype(np.uint8)
+    loss, g = ind.gradient(x, y, pos_weight=3.0)
+    lo, go = O.loss_and_grads(p.astype(np.float64), x, y, pos_weight=3.0)
+    assert abs(loss - lo) <= 1e-4 * abs(lo)
+    o = 0
+    for name, size in (("w1", O.HID * O.FEAT), ("b1", O.HID), ("w2", O.HID * O.HID),
+                       ("b2", O.HID), ("w3", O.HID), ("b3", 1)):
+        a, b = g[o:o + size], go[o:o + size]
+        rel = np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30)
+        assert rel <= 2e-2, (name, rel)
+        o += size
+
+
+def _ot_solver(n, order=5):
+    from quasar_b200 import ics, mhd
+    cfg = mhd.MhdConfig()
+    cfg.grid = mhd.Grid2D(n, n, 1.0, 1.0)
+    cfg.reconstruction = "mp5" if order == 5 else "mp7"
+    s = mhd.MhdSolver2D(cfg)
+    for name, a in zip(ics.COMPONENTS, ics.orszag_tang(n, order=order)):
+        s.seed_state(name, a)
+    return s
+
+
+def _state(s):
+    from quasar_b200 import ics
+    return [s.state_component_to_host(c) for c in ics.COMPONENTS]
+
+
+@pytest.mark.parametrize("order", [5, 7])
+def test_learned_mode_with_every_cell_flagged_is_the_plain_step(order):
+    from quasar_b200.indicator import TroubledCellIndicator, learned_face_counts
+    n = 48
+    a, b = _ot_solver(n, order), _ot_solver(n, order)
+    ind = TroubledCellIndicator(seed=1)
+    ind.attach(b, -1e30)
+    for _ in range(3):
+        a.step_unchecked(a.cfl_limit())
+        b.step_unchecked(b.cfl_limit())
+    ua, ub = _state(a), _state(b)
+    scale = max(np.max(np.abs(v)) for v in ua)
+    gap = max(np.max(np.abs(x - y)) for x, y in zip(ub, ua)) / scale
+    assert gap <= 1e-12, gap
+    ng = 3 if order == 5 else 4
+    fx, fy = learned_face_counts(b)
+    assert fx == (n + 1) * (n + 2 * ng) and fy == (n + 1) * (n + 2 * ng)
+
+
+def test_collect_train_and_learned_steps():
+    from quasar_b200.indicator import TroubledCellIndicator, learned_face_counts
+    n = 64
+    s = _ot_solver(n)
+    ind = TroubledCellIndicator(seed=2)
+    for k in range(40):
+        s.step_unchecked(s.cfl_limit())
+        if k % 4 == 3:
+            ind.collect(s)
+    assert ind.rows() == 10 * n * n
+    l0 = ind.train(epochs=1, tiles_per_step=16, lr=1e-3, pos_weight=4.0, holdout=10)
+    l1 = ind.train(epochs=6, tiles_per_step=16, lr=1e-3, pos_weight=4.0, holdout=10)
+    assert np.isfinite(l1) and l1 < l0
+    thr = ind.threshold_for_recall(0.99, holdout=10)
+    ev = ind.evaluate(thr, holdout=10)
+    assert ev["recall"] >= 0.99 and ev["positives"] > 0
+    # learned steps against plain ones from the same state
+    a, b = _ot_solver(n), _ot_solver(n)
+    for _ in range(30):
+        a.step_unchecked(a.cfl_limit())
+        b.step_unchecked(b.cfl_limit())
+    ind.attach(b, thr)
+    for _ in range(10):
+        a.step_unchecked(a.cfl_limit())
+        b.step_unchecked(b.cfl_limit())
+    fx, fy = learned_face_counts(b)
+    assert fx < (n + 1) * (n + 6)
+    ra, rb = _state(a)[0], _state(b)[0]
+    l1 = np.sum(np.abs(ra - rb)) / np.sum(np.abs(ra))
+    assert l1 <= 1e-3, l1
+    assert b.divergence_b_max() <= 1e-12

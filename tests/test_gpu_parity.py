@@ -161,3 +161,22 @@ def test_error_behaviour_matches_reference():
         g.step_unchecked(-1.0)
     with pytest.raises(ValueError):
         g.step(10.0 * g.cfl_limit())
+
+
+def test_orszag_tang_128_to_half_matches_reference_density():
+    """OT 128^2 MP5 to t = 0.5 through the device-resident loop against the
+    reference's own run (tests/golden/ot128_mp5_t05.npz): density L1 within
+    1e-6, the same number of steps, div B at the reference's own level."""
+    fx = load_fixture("ot128_mp5_t05")
+    n, order = 128, 5
+    g = gpu_solver(n, order)
+    seed(g, M.orszag_tang(n, order=order))
+    t, steps = g.advance_auto(0.0, 0.5, 100000)
+    assert t == 0.5
+    assert steps == len(fx["dts"])
+    ng = M.nghost(order)
+    rho = g.state_component_to_host("rho").reshape(n + 2 * ng, n + 2 * ng)[ng:-ng, ng:-ng]
+    ref = fx["rho"][ng:-ng, ng:-ng]
+    l1 = np.sum(np.abs(rho - ref)) / np.sum(np.abs(ref))
+    assert l1 <= 1e-6, l1
+    assert g.divergence_b_max() <= max(1e-12, 2.0 * float(fx["divb"]))
