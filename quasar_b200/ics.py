@@ -56,7 +56,7 @@ def rotor(n, order=7, gamma=5.0 / 3.0, ny=None, r0=0.1, bx=5.0 / math.sqrt(4.0 *
     X, Y = np.meshgrid(_centres(n, ng), _centres(ny, ng), indexing="xy")
     rx, ry = X - 0.5, Y - 0.5
     r = np.hypot(rx, ry)
-    r1, u0 = 1.15 * r0, 2.0
+    r1, u0 = 0.115 * (r0 / 0.1), 2.0  # 0.115 exactly at the default radius
     f = np.clip((r1 - r) / (r1 - r0), 0.0, 1.0)
     f = np.where(r <= r0, 1.0, np.where(r >= r1, 0.0, f))
     with np.errstate(divide="ignore", invalid="ignore"):
