@@ -19,6 +19,11 @@ in HBM; e2e = the same metric through the public C ABI with host buffers
 back); roofline = the reconstruction kernel (the largest share of the step)
 against the FP64 FMA peak measured on the same GPU; cpu_baseline = the
 reference's own MHD path built for the CPU, on a bounded sample.
+Beside the plain line: `learned` = the same workload with the shipped
+troubled-cell indicator (quasar_b200/data/indicator_mp{5,7}.npz), its speed-up
+and the density L1 gap to the plain run after the same steps; `batched` = 256
+seeded independent MP5 instances on uneven grids stepped together
+(--no-learned / --no-batch skip them).
 """
 from __future__ import annotations
 
@@ -65,6 +70,8 @@ def parse():
     ap.add_argument("--order", type=int, default=7, choices=[5, 7])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator run")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 256-instance batched run")
     return ap.parse_args()
 
 
@@ -293,6 +300,71 @@ def main():
                       "step_unchecked, state_component_to_host x8; host wall clock"}
         del s2
 
+    # the same workload with the learned troubled-cell indicator (shipped
+    # weights), from the same initial state and for the same number of steps,
+    # with the density L1 gap to the plain run
+    learned = None
+    if not a.no_learned:
+        from quasar_b200 import train_indicator
+        from quasar_b200.indicator import learned_face_counts
+        ind, thr = train_indicator.load(order=a.order)
+        s3 = make_solver(a)
+        seed(s3, comps)
+        ind.attach(s3, thr)
+
+        def timed3(k):
+            _native.check(L.qmhd_solver_time_auto_steps(s3._h, k, ctypes.byref(ms), ctypes.byref(done)))
+            if done.value != k:
+                raise RuntimeError(f"learned loop stopped after {done.value} of {k} steps")
+            return ms.value
+
+        timed3(max(a.warmup, 3))
+        dist.barrier()
+        tl = dist.reduce(timed3(a.steps), "max")
+        s3.step_unchecked(s3.cfl_limit())  # matches the profiled plain step
+        fx, fy = learned_face_counts(s3)
+        nfaces = (a.n + 1) * (a.n + 2 * ics.nghost(a.order))
+        r_plain = s.state_component_to_host("rho")
+        r_learn = s3.state_component_to_host("rho")
+        l1 = float(np.sum(np.abs(r_learn - r_plain)) / np.sum(np.abs(r_plain)))
+        learned = {"value": zones * a.steps * WORLD / (tl * 1e-3), "unit": "zone-updates/s",
+                   "ms_per_step": tl / a.steps, "speedup_vs_plain": t_ms / tl,
+                   "indicator": f"quasar_b200/data/indicator_mp{a.order}.npz",
+                   "threshold": thr, "full_path_face_fraction": (fx + fy) / (2.0 * nfaces),
+                   "rho_l1_vs_plain": l1, "steps_compared": max(a.warmup, 3) + a.steps + 1,
+                   "div_b_max": s3.divergence_b_max()}
+        del s3
+
+    # the batched plain step: 256 seeded independent MP5 instances on uneven
+    # grids, persistent per-phase launches in a CUDA graph, autotuned grids
+    batched = None
+    if not a.no_batch:
+        from quasar_b200 import mhd as _mhd
+        insts = ics.batch_instances(count=256, seed=0, order=5)
+        cfgs = []
+        for x in insts:
+            c = _mhd.MhdConfig()
+            c.grid = _mhd.Grid2D(x["nx"], x["ny"], x["lx"], x["ly"])
+            c.reconstruction = "mp5"
+            c.gamma = x["gamma"]
+            side = "periodic" if x["bc"] == 0 else "outflow"
+            c.boundary = _mhd.MhdBoundarySpec([side] * 4, [side] * 4)
+            cfgs.append(c)
+        b = _mhd.MhdBatch2D(cfgs)
+        for i, x in enumerate(insts):
+            for name, arr in zip(ics.COMPONENTS, x["arrays"]()):
+                b.instance(i).seed_state(name, arr)
+        ctas, trials = b.autotune()
+        b.time_steps(3)
+        bms, bzu = b.time_steps(max(10, a.steps // 10))
+        bms = dist.reduce(bms, "max")
+        batched = {"workload": "256 seeded MP5 instances, sides log-uniform in [64, 512], "
+                               "Orszag-Tang / oblique Brio-Wu / linear fast or Alfven waves",
+                   "zones": b.zones(), "value": bzu * WORLD / (bms * 1e-3), "unit": "zone-updates/s",
+                   "ms_per_step": bms / max(10, a.steps // 10), "autotuned_ctas_per_sm": ctas,
+                   "autotune_steps": trials}
+        del b
+
     cpu = None
     if RANK == 0 and WORLD == 1 and not a.no_cpu:
         cpu = reference_cpu(a.case, a.order, 3, 1)
@@ -307,7 +379,8 @@ def main():
                            "n": a.n, "order": a.order, "parallelism": f"replicas x{WORLD}",
                            "l2": "state 1 GB+ per register, larger than L2"},
                 "gpu_launches": LAUNCHES_PER_STEP * a.steps,
-                "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu}
+                "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "learned": learned, "batched": batched}
         print(json.dumps(line), flush=True)
     dist.close()
 

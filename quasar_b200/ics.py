@@ -304,25 +304,28 @@ def training_runs(count=12, seed=1, n=512, order=5):
     blast (radius in [0.05, 0.2], pressure ratio in [10, 1000], field in
     [0.1, 10]) and Orszag-Tang (field scale in [0.1, 10] as amplitude of B^2
     relative to the gas), cycled in that order.  Returns dicts with family,
-    parameters, bc and a zero-argument `arrays` callable."""
+    parameters, bc, a step budget that reaches the developed flow, and a
+    zero-argument `arrays` callable."""
     rng = np.random.default_rng(seed)
     lu = lambda a, b: float(math.exp(rng.uniform(math.log(a), math.log(b))))  # noqa: E731
     out = []
     for k in range(count):
         fam = ("rotor", "blast", "orszag_tang")[k % 3]
+        scale = n / 512.0  # steps to a comparable time at this resolution
         if fam == "rotor":
             r0, bf = lu(0.05, 0.2), lu(0.1, 10.0)
-            out.append(dict(family=fam, radius=r0, field=bf, bc=1,
+            out.append(dict(family=fam, radius=r0, field=bf, bc=1, steps=int(1200 * scale),
                             arrays=lambda r0=r0, bf=bf: rotor(n, order=order, r0=r0, bx=bf)))
         elif fam == "blast":
             r0, ratio, bf = lu(0.05, 0.2), lu(10.0, 1000.0), lu(0.1, 10.0)
             out.append(dict(family=fam, radius=r0, ratio=ratio, field=bf, bc=1,
+                            steps=int(1200 * scale),
                             arrays=lambda r0=r0, ratio=ratio, bf=bf: blast(
                                 n, order=order, radius=r0, p_in=0.1 * ratio, p_out=0.1,
                                 b=bf / math.sqrt(2.0))))
         else:
             amp = lu(0.1, 10.0)
-            out.append(dict(family=fam, field=amp, bc=0,
+            out.append(dict(family=fam, field=amp, bc=0, steps=int(4000 * scale),
                             arrays=lambda amp=amp: _ot_field_scaled(n, order, amp)))
     return out
 

@@ -3,8 +3,8 @@
     python -m quasar_b200.train_indicator --out quasar_b200/data/indicator_mp5.npz
 
 Labels come from plain-method runs of the seeded rotor / blast / Orszag-Tang
-families of `quasar_b200.ics.training_runs`: every `every` steps the live
-state of each run is collected (features of every interior cell and whether
+families of `quasar_b200.ics.training_runs`: evenly spaced live states of
+each run are collected (features of every interior cell and whether
 its limited characteristic face states depart from the component-wise
 unlimited ones), then Adam trains the network with the tensor-core
 forward/backward kernels.  The threshold is the smallest logit that keeps
@@ -32,13 +32,16 @@ def _solver(n, order, bc):
     return mhd.MhdSolver2D(cfg)
 
 
-def collect(ind, n=512, runs=12, steps=400, every=20, order=5, seed=1, tol=1e-6, log=print):
+def collect(ind, n=512, runs=12, snapshots=20, order=5, seed=1, tol=1e-6, log=print):
+    """Step each seeded run through its step budget, collecting `snapshots`
+    evenly spaced live states."""
     t0 = time.time()
     for k, run in enumerate(ics.training_runs(count=runs, seed=seed, n=n, order=order)):
         s = _solver(n, order, run["bc"])
         for name, a in zip(ics.COMPONENTS, run["arrays"]()):
             s.seed_state(name, a)
         t, done = 0.0, 0
+        steps, every = run["steps"], max(1, run["steps"] // snapshots)
         while done < steps:
             try:
                 t, taken = s.advance_auto(t, 1e30, every)
@@ -52,23 +55,23 @@ def collect(ind, n=512, runs=12, steps=400, every=20, order=5, seed=1, tol=1e-6,
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "data", "indicator_mp5.npz"))
+    ap.add_argument("--out", default=None)
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--runs", type=int, default=12)
-    ap.add_argument("--steps", type=int, default=400)
-    ap.add_argument("--every", type=int, default=20)
+    ap.add_argument("--snapshots", type=int, default=20)
     ap.add_argument("--order", type=int, default=5)
-    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=10)
     ap.add_argument("--tiles", type=int, default=512)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--pos-weight", type=float, default=8.0)
-    ap.add_argument("--recall", type=float, default=0.995)
+    ap.add_argument("--pos-weight", type=float, default=30.0)
+    ap.add_argument("--recall", type=float, default=0.99)
     ap.add_argument("--holdout", type=int, default=20)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--tol", type=float, default=1e-5)
     a = ap.parse_args(argv)
+    a.out = a.out or default_path(a.order)
     ind = TroubledCellIndicator(seed=a.seed)
-    collect(ind, a.n, a.runs, a.steps, a.every, a.order, a.seed, a.tol)
+    collect(ind, a.n, a.runs, a.snapshots, a.order, a.seed, a.tol)
     t0 = time.time()
     losses = []
     for ep in range(a.epochs):
@@ -86,9 +89,13 @@ def main(argv=None):
     return ind, thr, ev
 
 
-def load(path=None):
+def default_path(order):
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", f"indicator_mp{order}.npz")
+
+
+def load(path=None, order=5):
     """(indicator, threshold) from a file written by main()."""
-    path = path or os.path.join(os.path.dirname(__file__), "data", "indicator_mp5.npz")
+    path = path or default_path(order)
     z = np.load(path)
     ind = TroubledCellIndicator(seed=0)
     ind.set_params(z["params"])
