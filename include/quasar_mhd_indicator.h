@@ -80,6 +80,12 @@ int qmhd_indicator_threshold_for_recall(qmhd_indicator* ind, double recall, int 
  * equals the characteristic result wherever the limiter would not fire.
  * ind = NULL restores the plain step.  The indicator must outlive this use. */
 int qmhd_solver_set_indicator(qmhd_solver* solver, const qmhd_indicator* ind, float threshold);
+/* The same learned mode for every instance of a batch (quasar_mhd_batch.h):
+ * one batched indicator launch per step over all instances, their face lists
+ * and the two reconstruction passes inside the batched step. */
+struct qmhd_batch;
+int qmhd_batch_set_indicator(struct qmhd_batch* batch, const qmhd_indicator* ind,
+                             float threshold);
 /* Faces on the full-reconstruction lists of the last learned step. */
 int qmhd_solver_learned_face_counts(qmhd_solver* solver, long long* x_faces, long long* y_faces);
 

@@ -34,7 +34,7 @@ INDICATOR_EXPORTS = ("qmhd_indicator_create", "qmhd_indicator_destroy", "qmhd_in
                      "qmhd_indicator_gradient", "qmhd_indicator_collect", "qmhd_indicator_rows",
                      "qmhd_indicator_clear", "qmhd_indicator_train", "qmhd_indicator_evaluate",
                      "qmhd_indicator_threshold_for_recall", "qmhd_solver_set_indicator",
-                     "qmhd_solver_learned_face_counts")
+                     "qmhd_solver_learned_face_counts", "qmhd_batch_set_indicator")
 
 
 class QmhdConfig(ctypes.Structure):
@@ -114,6 +114,7 @@ def lib() -> ctypes.CDLL:
     L.qmhd_indicator_threshold_for_recall.argtypes = [vp, ctypes.c_double, ctypes.c_int,
                                                       ctypes.POINTER(ctypes.c_float)]
     L.qmhd_solver_set_indicator.argtypes = [vp, vp, ctypes.c_float]
+    L.qmhd_batch_set_indicator.argtypes = [vp, vp, ctypes.c_float]
     L.qmhd_solver_learned_face_counts.argtypes = [vp, lp, lp]
     _lib = L
     return L

@@ -301,6 +301,13 @@ int qmhd_batch_set_tuning(qmhd_batch* batch, const int* ctas_per_sm) {
 
 long long qmhd_batch_zones(const qmhd_batch* batch) { return batch ? batch->impl->zones() : -1; }
 
+int qmhd_batch_set_indicator(qmhd_batch* batch, const qmhd_indicator* ind, float threshold) {
+  return guarded([&] {
+    need(batch);
+    batch->impl->set_indicator(ind ? &ind->impl : nullptr, threshold);
+  });
+}
+
 static_assert(QMHD_BATCH_PHASES == qb::kBpCount, "phase count");
 
 // ---- learned troubled-cell indicator (include/quasar_mhd_indicator.h) -----

@@ -503,9 +503,49 @@ struct InfSmem {
 // One 16 x 8 block of padded cells per tile: primitives of its 20 x 12 halo
 // into shared memory, each thread's feature row straight into the
 // tensor-core operand layout, then the two MMAs and the head.
-__global__ void __launch_bounds__(kThreads) k_indicator(Grid g, StateP u, double gamma, MlpDev p,
-                                                        float thr, unsigned char* __restrict__ flag,
-                                                        int* status) {
+// Tile sources: one state, or every instance of a batch (live state, stage-0
+// records, learned buffers).
+struct SingleSrc {
+  Grid g;
+  StateP u;
+  double gamma;
+  unsigned char* flag;
+  __device__ long long tiles() const {
+    return (long long)((g.pitch + kTileX - 1) / kTileX) * ((g.ny + 2 * g.ng + kTileY - 1) / kTileY);
+  }
+  __device__ void get(long long t, const Grid** gg, const StateP** uu, double* ga,
+                      unsigned char** fl, int* i0, int* j0) const {
+    const int ntx = (g.pitch + kTileX - 1) / kTileX;
+    *gg = &g;
+    *uu = &u;
+    *ga = gamma;
+    *fl = flag;
+    *i0 = int(t % ntx) * kTileX - g.ng;
+    *j0 = int(t / ntx) * kTileY - g.ng;
+  }
+};
+struct BatchSrc {
+  const BatchRec* r;
+  const BatchLearnRec* l;
+  BatchPlan p;
+  __device__ long long tiles() const { return p.total; }
+  __device__ void get(long long t, const Grid** gg, const StateP** uu, double* ga,
+                      unsigned char** fl, int* i0, int* j0) const {
+    int local, bx, by;
+    const int inst = batch_locate(p, int(t), &local);
+    const BatchRec& q = r[inst];
+    batch_block(kBpInd, q.a.g, local, &bx, &by);
+    *gg = &q.a.g;
+    *uu = &q.a.u;
+    *ga = q.a.gamma;
+    *fl = l[inst].flag;
+    *i0 = bx * kTileX - q.a.g.ng;
+    *j0 = by * kTileY - q.a.g.ng;
+  }
+};
+
+template <class Src>
+__global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float thr, int* status) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint8_t* xs = sm;
   uint8_t* w1s = xs + InfSmem::kX;
@@ -529,13 +569,18 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Grid g, StateP u, double
   tc::fence_after_sync();
   const uint32_t tb = *tslot;
   const uint32_t idesc = tc::idesc_bf16(128, kHidden);
-  const int ntx = (g.pitch + kTileX - 1) / kTileX;
-  const long long tiles = (long long)ntx * ((g.ny + 2 * g.ng + kTileY - 1) / kTileY);
+  const long long tiles = src.tiles();
   uint32_t phase = 0;
   bool ok = true;
   for (long long t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-    const int i0 = int(t % ntx) * kTileX - g.ng;
-    const int j0 = int(t / ntx) * kTileY - g.ng;
+    const Grid* gp;
+    const StateP* up;
+    double gamma;
+    unsigned char* flag;
+    int i0, j0;
+    src.get(t, &gp, &up, &gamma, &flag, &i0, &j0);
+    const Grid& g = *gp;
+    const StateP& u = *up;
     for (int e = tid; e < kHaloX * kHaloY; e += kThreads) {
       const int rr = e / kHaloX, cc = e - rr * kHaloX;
       const int ci = i0 - 2 + cc, cj = j0 - 2 + rr;
@@ -706,7 +751,10 @@ void launch_adam(float* params, float* m, float* v, const float* grad, int step,
 }
 
 cudaError_t configure_indicator_kernels() {
-  return cudaFuncSetAttribute(k_indicator, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_indicator<SingleSrc>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, InfSmem::kTotal);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_indicator<BatchSrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               InfSmem::kTotal);
 }
 
@@ -715,7 +763,17 @@ cudaError_t launch_indicator(const Grid& g, const StateP& u, double gamma, const
   const long long tiles = (long long)((g.pitch + kTileX - 1) / kTileX) *
                           ((g.ny + 2 * g.ng + kTileY - 1) / kTileY);
   const int grid = int(tiles < 2 * sm_count() ? tiles : 2 * sm_count());
-  k_indicator<<<grid, kThreads, InfSmem::kTotal, s>>>(g, u, gamma, p, threshold, flag, status);
+  SingleSrc src{g, u, gamma, flag};
+  k_indicator<SingleSrc><<<grid, kThreads, InfSmem::kTotal, s>>>(src, p, threshold, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_indicator(const BatchRec* r, const BatchLearnRec* l, const BatchPlan& plan,
+                                   const MlpDev& p, float threshold, int* status, cudaStream_t s) {
+  const int grid = int(plan.total < 2 * sm_count() ? plan.total : 2 * sm_count());
+  if (grid <= 0) return cudaSuccess;
+  BatchSrc src{r, l, plan};
+  k_indicator<BatchSrc><<<grid, kThreads, InfSmem::kTotal, s>>>(src, p, threshold, status);
   return cudaGetLastError();
 }
 

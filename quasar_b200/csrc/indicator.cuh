@@ -79,6 +79,10 @@ void launch_adam(float* params, float* m, float* v, const float* grad, int step,
 // Kernel attributes of launch_indicator; call once before it is launched or
 // captured into a graph.
 cudaError_t configure_indicator_kernels();
+// The same over the stage-0 (live) records of a batch, one learned buffer
+// set per instance; plan = the kBpInd tile plan.
+cudaError_t launch_batch_indicator(const BatchRec* r, const BatchLearnRec* l, const BatchPlan& plan,
+                                   const MlpDev& p, float threshold, int* status, cudaStream_t s);
 cudaError_t launch_indicator(const Grid& g, const StateP& u, double gamma, const MlpDev& p,
                              float threshold, unsigned char* flag, int* status, cudaStream_t s);
 

@@ -1,5 +1,6 @@
 // Batched MHD step (see mhd_batch.cuh).
 #include "mhd_batch.cuh"
+#include "indicator.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -50,7 +51,7 @@ MhdBatch2D::MhdBatch2D(const std::vector<Config>& configs) {
   ck(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev), "SM count");
   ck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
   ck(cudaMalloc(&recs_, sizeof(BatchRec) * 6 * size_t(n)), "batch records");
-  ck(cudaMalloc(&prefix_, sizeof(int) * kBpCount * size_t(n + 1)), "batch plans");
+  ck(cudaMalloc(&prefix_, sizeof(int) * kBpAll * size_t(n + 1)), "batch plans");
   max_ctas_.resize(kBpCount);
   ctas_per_sm_.resize(kBpCount);
   for (int ph = 0; ph < kBpCount; ++ph) {
@@ -65,6 +66,8 @@ MhdBatch2D::~MhdBatch2D() {
   if (stream_) cudaStreamSynchronize(stream_);
   cudaFree(recs_);
   cudaFree(prefix_);
+  cudaFree(learn_);
+  cudaFree(ind_status_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -87,8 +90,8 @@ void MhdBatch2D::set_tuning(const std::vector<int>& ctas) {
 
 void MhdBatch2D::build_plans() {
   const int n = size();
-  std::vector<int> h(size_t(kBpCount) * (n + 1));
-  for (int ph = 0; ph < kBpCount; ++ph) {
+  std::vector<int> h(size_t(kBpAll) * (n + 1));
+  for (int ph = 0; ph < kBpAll; ++ph) {
     int* p = h.data() + size_t(ph) * (n + 1);
     long long acc = 0;
     for (int s = 0; s < n; ++s) {
@@ -101,7 +104,7 @@ void MhdBatch2D::build_plans() {
       throw std::invalid_argument("MhdBatch2D: batch too large for one launch");
     p[n] = int(acc);
     const int total = int(acc);
-    const int c = ctas_per_sm_[size_t(ph)];
+    const int c = ph < kBpCount ? ctas_per_sm_[size_t(ph)] : 0;
     plan_[ph].prefix = prefix_ + size_t(ph) * (n + 1);
     plan_[ph].n = n;
     plan_[ph].total = total;
@@ -140,6 +143,27 @@ void MhdBatch2D::build_tables() {
   ck(cudaStreamSynchronize(stream_), "records");
 }
 
+void MhdBatch2D::set_indicator(const Indicator* ind, float threshold) {
+  if (ind && !ind_status_) {
+    ck(cudaMalloc(&ind_status_, sizeof(int)), "indicator status");
+    ck(cudaMemset(ind_status_, 0, sizeof(int)), "indicator status");
+    ck(cudaMalloc(&learn_, sizeof(BatchLearnRec) * size_t(size())), "learned records");
+  }
+  for (auto& m : inst_) m->set_indicator(ind, threshold);
+  if (ind) {
+    std::vector<BatchLearnRec> h(static_cast<size_t>(size()));
+    for (int s = 0; s < size(); ++s) {
+      MhdSolver2D& m = *inst_[size_t(slot_[size_t(s)])];
+      h[size_t(s)] = BatchLearnRec{m.flags_, m.flists_, m.flists_ + m.g_.size(), m.fcounts_};
+    }
+    ck(cudaMemcpy(learn_, h.data(), sizeof(BatchLearnRec) * h.size(), cudaMemcpyHostToDevice),
+       "learned records");
+  }
+  ind_ = ind;
+  ind_threshold_ = threshold;
+  release_graphs();
+}
+
 void MhdBatch2D::prepare() {
   for (auto& m : inst_) {
     m->ensure_live_ready();
@@ -164,13 +188,29 @@ void MhdBatch2D::enqueue_step(int par, std::vector<cudaEvent_t>* marks,
   };
   launch_batch_ctl(recs(par, 0), n, 0, 0.0, 0.0, stream_);
   mark(-1);
+  if (ind_) {
+    // score every instance's live state once per step
+    launch_batch_learned_reset(recs(par, 0), learn_, plan_[kBpCells], stream_);
+    ck(launch_batch_indicator(recs(par, 0), learn_, plan_[kBpInd], ind_->dev(), ind_threshold_,
+                              ind_status_, stream_),
+       "batched indicator");
+    launch_batch_face_lists(recs(par, 0), learn_, plan_[kBpCells], stream_);
+    mark(-1);
+  }
   for (int st = 0; st < 3; ++st) {
     const BatchRec* r = recs(par, st);
     const bool first = st == 0;
-    launch_batch_reconstruct(r, plan_[kBpRecon0], 0, order_, stream_);
-    mark(kBpRecon0);
-    launch_batch_reconstruct(r, plan_[kBpRecon1], 1, order_, stream_);
-    mark(kBpRecon1);
+    if (ind_) {
+      launch_batch_reconstruct_learned(r, learn_, plan_[kBpRecon0], 0, order_, 2 * sms_, stream_);
+      mark(kBpRecon0);
+      launch_batch_reconstruct_learned(r, learn_, plan_[kBpRecon1], 1, order_, 2 * sms_, stream_);
+      mark(kBpRecon1);
+    } else {
+      launch_batch_reconstruct(r, plan_[kBpRecon0], 0, order_, stream_);
+      mark(kBpRecon0);
+      launch_batch_reconstruct(r, plan_[kBpRecon1], 1, order_, stream_);
+      mark(kBpRecon1);
+    }
     launch_batch_face_flux(r, plan_[kBpFlux], 0, order_, first, stream_);
     launch_batch_face_flux(r, plan_[kBpFlux], 1, order_, first, stream_);
     mark(kBpFlux);

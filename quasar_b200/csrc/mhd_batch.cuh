@@ -46,6 +46,11 @@ class MhdBatch2D {
   const std::vector<int>& tuning() const { return ctas_per_sm_; }
   void set_tuning(const std::vector<int>& ctas_per_sm);
 
+  // Learned troubled-cell mode for every instance (batched indicator, face
+  // lists and two-pass reconstruction inside the batched step); nullptr
+  // returns to the plain step.  The indicator must outlive its use.
+  void set_indicator(const Indicator* ind, float threshold);
+
  private:
   void prepare();                 // instance preflights, tables, plans
   void build_tables();
@@ -65,10 +70,15 @@ class MhdBatch2D {
   cudaStream_t stream_ = nullptr;
   BatchRec* recs_ = nullptr;      // device [parity 2][stage 3][slot]
   int* prefix_ = nullptr;         // device [phase][slot + 1]
-  BatchPlan plan_[kBpCount];
+  BatchPlan plan_[kBpAll];
   std::vector<int> ctas_per_sm_;  // per phase
   std::vector<int> max_ctas_;     // per phase, occupancy limit
   cudaGraphExec_t graph_[2] = {nullptr, nullptr};
+  // learned mode
+  const Indicator* ind_ = nullptr;
+  float ind_threshold_ = 0.f;
+  BatchLearnRec* learn_ = nullptr;  // device, slot order
+  int* ind_status_ = nullptr;
 };
 
 }  // namespace qb

@@ -197,7 +197,23 @@ __device__ __forceinline__ double convex_q(const St& a, const St& b, double th) 
   const double q = (e - kin_mom(mx, my, mz, rho)) - half_sq3(bx, by, bz);
   return isfinite(q) ? q : -kInf;
 }
+// Internal energy certainly positive: plain arithmetic with a margin far
+// above its rounding error (a few ulps of E + kinetic + magnetic), so the
+// sign agrees with the reference's scaled form whenever this returns true.
+__device__ __forceinline__ bool surely_admissible(const St& s) {
+  if (!(isfinite(s.rho) && s.rho > 0.0 && isfinite(s.mx) && isfinite(s.my) && isfinite(s.mz) &&
+        isfinite(s.E) && isfinite(s.bx) && isfinite(s.by) && isfinite(s.bz)))
+    return false;
+  const double kin = 0.5 * ((s.mx * s.mx + s.my * s.my + s.mz * s.mz) / s.rho);
+  const double mag = 0.5 * (s.bx * s.bx + s.by * s.by + s.bz * s.bz);
+  const double q = (s.E - kin) - mag;
+  return isfinite(q) && q > 1e-12 * (fabs(s.E) + kin + mag);
+}
+
 __device__ double admissible_fraction(const St& a, const St& b) {
+  // both end points certainly admissible: the exact path returns 1 as well
+  // (convex_q at theta 0 and 1 are the end points themselves)
+  if (surely_admissible(a) && surely_admissible(b)) return 1.0;
   const double qa = convex_q(a, b, 0.0);
   if (!(a.rho > 0.0) || !(qa > 0.0) || !isfinite(a.rho) || !isfinite(qa)) return 0.0;
   if (!(isfinite(b.rho) && isfinite(b.mx) && isfinite(b.my) && isfinite(b.mz) &&
@@ -1686,32 +1702,76 @@ __global__ void k_cell_sums(Grid g, StateP u, double* partial) {
 // ===========================================================================
 namespace {
 
-__device__ __forceinline__ int batch_locate(const BatchPlan& p, int t, int* local) {
-  int lo = 0, hi = p.n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(p.prefix + mid) <= t) lo = mid;
-    else hi = mid - 1;
-  }
-  *local = t - __ldg(p.prefix + lo);
-  return lo;
-}
-
-__device__ __forceinline__ void batch_block(int phase, const Grid& g, int local, int* bx, int* by) {
-  int tx, ty;
-  batch_tiles(phase, g, &tx, &ty);
-  *bx = local % tx;
-  *by = local / tx;
-}
-
-template <int DIR, int ORDER>
+template <int DIR, int ORDER, int MODE = 0>
 __global__ void __launch_bounds__(128) kb_reconstruct(const BatchRec* __restrict__ r, BatchPlan p) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
     int local, bx, by;
     const BatchRec& q = r[batch_locate(p, t, &local)];
     batch_block(DIR == 0 ? kBpRecon0 : kBpRecon1, q.a.g, local, &bx, &by);
-    b_reconstruct<DIR, ORDER>(q.a.g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma, q.a.ctl, bx,
-                              by);
+    b_reconstruct<DIR, ORDER, MODE>(q.a.g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma,
+                                    q.a.ctl, bx, by);
+  }
+}
+
+// Characteristic pass over every instance's face list: each CTA takes its
+// share of each instance's list in turn.
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128) kb_reconstruct_list(const BatchRec* __restrict__ r,
+                                                           const BatchLearnRec* __restrict__ l,
+                                                           int n) {
+  for (int inst = 0; inst < n; ++inst) {
+    const BatchRec& q = r[inst];
+    if (q.a.ctl->status & ~kStatusDone) continue;
+    const int cnt = l[inst].counts[DIR];
+    const int* list = DIR == 0 ? l[inst].xlist : l[inst].ylist;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+      const int k = list[t];
+      const int i = k % q.a.g.pitch - q.a.g.ng, j = k / q.a.g.pitch - q.a.g.ng;
+      recon_face<DIR, ORDER, 0>(q.a.g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma, i, j,
+                                nullptr);
+    }
+  }
+}
+
+__global__ void kb_learned_reset(const BatchRec* __restrict__ r, const BatchLearnRec* __restrict__ l,
+                                 BatchPlan p) {
+  for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
+    int local;
+    const int inst = batch_locate(p, t, &local);
+    const long long k = (long long)local * 256 + threadIdx.x;
+    if (k < r[inst].a.g.size()) l[inst].flag[k] = 1;
+    if (local == 0 && threadIdx.x < 2) l[inst].counts[threadIdx.x] = 0;
+  }
+}
+
+// k_face_lists over 256-cell chunks of every instance.
+__global__ void kb_face_lists(const BatchRec* __restrict__ r, const BatchLearnRec* __restrict__ l,
+                              BatchPlan p) {
+  for (int tt = blockIdx.x; tt < p.total; tt += gridDim.x) {
+    int local;
+    const int inst = batch_locate(p, tt, &local);
+    const Grid& g = r[inst].a.g;
+    const BatchLearnRec& L = l[inst];
+    const long long t = (long long)local * 256 + threadIdx.x;
+    const unsigned lane = threadIdx.x & 31;
+    bool nx_ = false, ny_ = false;
+    const int k = int(t);
+    if (t < g.size()) {
+      const int i = int(t % g.pitch) - g.ng, j = int(t / g.pitch) - g.ng;
+      if (i >= 0 && i <= g.nx && j < g.ny + g.ng) nx_ = (L.flag[t] | L.flag[t - 1]) != 0;
+      if (j >= 0 && j <= g.ny && i < g.nx + g.ng) ny_ = (L.flag[t] | L.flag[t - g.pitch]) != 0;
+    }
+    const unsigned bx_ = __ballot_sync(0xffffffffu, nx_), by_ = __ballot_sync(0xffffffffu, ny_);
+    int basex = 0, basey = 0;
+    if (lane == 0) {
+      if (bx_) basex = atomicAdd(&L.counts[0], __popc(bx_));
+      if (by_) basey = atomicAdd(&L.counts[1], __popc(by_));
+    }
+    basex = __shfl_sync(0xffffffffu, basex, 0);
+    basey = __shfl_sync(0xffffffffu, basey, 0);
+    const unsigned below = (1u << lane) - 1u;
+    if (nx_) L.xlist[basex + __popc(bx_ & below)] = k;
+    if (ny_) L.ylist[basey + __popc(by_ & below)] = k;
   }
 }
 
@@ -2060,6 +2120,39 @@ void launch_batch_colloc_check(const BatchRec* r, const BatchPlan& p, int order,
   const dim3 block(32, 8);
   if (order == 7) kb_colloc_check<8><<<pgrid(p), block, 0, s>>>(r, p, theta_mask, live_checks ? 1 : 0);
   else kb_colloc_check<6><<<pgrid(p), block, 0, s>>>(r, p, theta_mask, live_checks ? 1 : 0);
+}
+
+void launch_batch_learned_reset(const BatchRec* r, const BatchLearnRec* l, const BatchPlan& cells,
+                                cudaStream_t s) {
+  kb_learned_reset<<<pgrid(cells), 256, 0, s>>>(r, l, cells);
+}
+
+void launch_batch_face_lists(const BatchRec* r, const BatchLearnRec* l, const BatchPlan& cells,
+                             cudaStream_t s) {
+  kb_face_lists<<<pgrid(cells), 256, 0, s>>>(r, l, cells);
+}
+
+void launch_batch_reconstruct_learned(const BatchRec* r, const BatchLearnRec* l,
+                                      const BatchPlan& p, int dir, int order, int list_grid,
+                                      cudaStream_t s) {
+  const dim3 block(32, 4);
+  if (order == 7) {
+    if (dir == 0) {
+      kb_reconstruct<0, 7, 2><<<pgrid(p), block, 0, s>>>(r, p);
+      kb_reconstruct_list<0, 7><<<list_grid, 128, 0, s>>>(r, l, p.n);
+    } else {
+      kb_reconstruct<1, 7, 2><<<pgrid(p), block, 0, s>>>(r, p);
+      kb_reconstruct_list<1, 7><<<list_grid, 128, 0, s>>>(r, l, p.n);
+    }
+  } else {
+    if (dir == 0) {
+      kb_reconstruct<0, 5, 2><<<pgrid(p), block, 0, s>>>(r, p);
+      kb_reconstruct_list<0, 5><<<list_grid, 128, 0, s>>>(r, l, p.n);
+    } else {
+      kb_reconstruct<1, 5, 2><<<pgrid(p), block, 0, s>>>(r, p);
+      kb_reconstruct_list<1, 5><<<list_grid, 128, 0, s>>>(r, l, p.n);
+    }
+  }
 }
 
 void launch_batch_ctl(const BatchRec* r, int n, int what, double t, double t_end, cudaStream_t s) {

@@ -128,6 +128,18 @@ enum BatchPhase : int {
   kBpRecon0, kBpRecon1, kBpFlux, kBpCell, kBpCorner, kBpUpdate, kBpColloc, kBpFill0, kBpFill1,
   kBpCount
 };
+// Extra tile phases of the learned batched step (not autotuned): indicator
+// tiles of 16 x 8 padded cells, and 256-cell chunks of the padded grid.
+enum : int { kBpInd = kBpCount, kBpCells = kBpCount + 1, kBpAll = kBpCount + 2 };
+
+// Learned-mode buffers of one instance (those of its MhdSolver2D).
+struct BatchLearnRec {
+  unsigned char* flag;  // per padded cell
+  int* xlist;
+  int* ylist;
+  int* counts;          // [2]
+};
+
 struct BatchPlan {
   const int* prefix;  // device, n + 1 entries
   int n;              // instances
@@ -148,9 +160,33 @@ __host__ __device__ inline void batch_tiles(int phase, const Grid& g, int* tx, i
     case kBpUpdate: *tx = cd(g.nx + 1, 32); *ty = cd(g.ny + 1, 8); break;
     case kBpColloc: *tx = cd(g.nx + 2 * g.ng, 32); *ty = cd(g.ny + 2 * g.ng, 8); break;
     case kBpFill0: *tx = cd(2 * g.ng * (g.ny + 2 * g.ng), 256); *ty = 1; break;
-    default: *tx = cd(2 * g.ng * (g.nx + 2 * g.ng), 256); *ty = 1; break;
+    case kBpFill1: *tx = cd(2 * g.ng * (g.nx + 2 * g.ng), 256); *ty = 1; break;
+    case kBpInd: *tx = cd(g.pitch, 16); *ty = cd(g.ny + 2 * g.ng, 8); break;
+    default: *tx = int((g.size() + 255) / 256); *ty = 1; break;  // kBpCells
   }
 }
+
+#ifdef __CUDACC__
+// Instance of global tile t (largest i with prefix[i] <= t) and the tile's
+// index within that instance.
+__device__ __forceinline__ int batch_locate(const BatchPlan& p, int t, int* local) {
+  int lo = 0, hi = p.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(p.prefix + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  *local = t - __ldg(p.prefix + lo);
+  return lo;
+}
+
+__device__ __forceinline__ void batch_block(int phase, const Grid& g, int local, int* bx, int* by) {
+  int tx, ty;
+  batch_tiles(phase, g, &tx, &ty);
+  *bx = local % tx;
+  *by = local / tx;
+}
+#endif
 
 // Threads per CTA of each phase's batched kernel and its resident CTAs per SM
 // (queried once per process), for sizing persistent grids.
@@ -170,6 +206,17 @@ void launch_batch_update(const BatchRec* r, const BatchPlan& p, int stage, cudaS
 void launch_batch_fill_ghosts(const BatchRec* r, const BatchPlan& p, int axis, cudaStream_t s);
 void launch_batch_colloc_check(const BatchRec* r, const BatchPlan& p, int order, int theta_mask,
                                bool live_checks, cudaStream_t s);
+// Learned batched step: flags of every padded cell set to 1 and list counts
+// cleared (cells plan), face lists of every instance, and the two
+// reconstruction passes (component-wise over all faces, characteristic over
+// each instance's list).
+void launch_batch_learned_reset(const BatchRec* r, const BatchLearnRec* l, const BatchPlan& cells,
+                                cudaStream_t s);
+void launch_batch_face_lists(const BatchRec* r, const BatchLearnRec* l, const BatchPlan& cells,
+                             cudaStream_t s);
+void launch_batch_reconstruct_learned(const BatchRec* r, const BatchLearnRec* l,
+                                      const BatchPlan& p, int dir, int order, int list_grid,
+                                      cudaStream_t s);
 // Per-instance control kernels (one thread per instance): 0 step_begin
 // (collocation 0, anchor from the live state), 1 dt (clipped to t_end),
 // 2 step_end, 3 set_time(t, t_end).

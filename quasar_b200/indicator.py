@@ -96,6 +96,13 @@ class TroubledCellIndicator:
         solver._indicator = self
 
 
+def attach_batch(ind, batch, threshold: float) -> None:
+    """Learned mode for every instance of an MhdBatch2D (kept alive by it)."""
+    _native.check(_native.lib().qmhd_batch_set_indicator(batch._h, ind._h,
+                                                         ctypes.c_float(threshold)))
+    batch._indicator = ind
+
+
 def detach(solver) -> None:
     """Back to the plain step."""
     _native.check(_native.lib().qmhd_solver_set_indicator(solver._h, None, ctypes.c_float(0.0)))

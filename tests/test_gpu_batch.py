@@ -124,3 +124,46 @@ def test_oblique_families_match_oracle(oracle, family):
         err = M.state_rel_l1(read_all(g, inst, order), o.read(), ng, nx, ny)
         assert err <= STEP_TOL, (k, err)
     assert g.divergence_b_max() <= 1e-12
+
+
+def _seeded_pair(order, count, seed):
+    insts = mixed_instances(order, count=count, seed=seed)
+    b = mhd.MhdBatch2D([config(x, order) for x in insts])
+    c = mhd.MhdBatch2D([config(x, order) for x in insts])
+    for i, x in enumerate(insts):
+        arrays = x["arrays"]()
+        for name, a in zip(ics.COMPONENTS, arrays):
+            b.instance(i).seed_state(name, a)
+            c.instance(i).seed_state(name, a)
+    return insts, b, c
+
+
+def test_batched_learned_with_every_cell_flagged_is_the_batched_step():
+    from quasar_b200.indicator import TroubledCellIndicator, attach_batch
+    order = 5
+    insts, b, c = _seeded_pair(order, 5, 21)
+    ind = TroubledCellIndicator(seed=3)
+    attach_batch(ind, c, -1e30)
+    assert b.advance(4) == [4] * len(insts)
+    assert c.advance(4) == [4] * len(insts)
+    for i, x in enumerate(insts):
+        err = rounding_gap(read_all(c.instance(i), x, order), read_all(b.instance(i), x, order))
+        assert err <= BATCH_TOL, (x["family"], i, err)
+
+
+def test_batched_learned_with_shipped_indicator_stays_close():
+    from quasar_b200 import train_indicator
+    from quasar_b200.indicator import attach_batch
+    order = 5
+    insts, b, c = _seeded_pair(order, 6, 22)
+    ind, thr = train_indicator.load(order=order)
+    attach_batch(ind, c, thr)
+    b.advance(20)
+    c.advance(20)
+    ng = ics.nghost(order)
+    for i, x in enumerate(insts):
+        rb = read_all(b.instance(i), x, order)[0][ng:-ng, ng:-ng]
+        rc = read_all(c.instance(i), x, order)[0][ng:-ng, ng:-ng]
+        l1 = np.sum(np.abs(rc - rb)) / np.sum(np.abs(rb))
+        assert l1 <= 1e-4, (x["family"], i, l1)
+        assert c.instance(i).divergence_b_max() <= 1e-11
