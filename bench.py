@@ -22,8 +22,9 @@ reference's own MHD path built for the CPU, on a bounded sample.
 Beside the plain line: `learned` = the same workload with the shipped
 troubled-cell indicator (quasar_b200/data/indicator_mp{5,7}.npz), its speed-up
 and the density L1 gap to the plain run after the same steps; `batched` = 256
-seeded independent MP5 instances on uneven grids stepped together
-(--no-learned / --no-batch skip them).
+seeded independent MP5 instances on uneven grids stepped together;
+`batched_learned` = one batch of Orszag-Tang 8192^2 MP7 and 64 rotor/blast
+instances, plain and then learned (--no-learned / --no-batch skip them).
 """
 from __future__ import annotations
 
@@ -199,6 +200,29 @@ def make_solver(a):
     return mhd.MhdSolver2D(cfg)
 
 
+def make_batch(insts, order):
+    from quasar_b200 import mhd
+    cfgs = []
+    for x in insts:
+        c = mhd.MhdConfig()
+        c.grid = mhd.Grid2D(x["nx"], x["ny"], x["lx"], x["ly"])
+        c.reconstruction = "mp7" if order == 7 else "mp5"
+        c.gamma = x["gamma"]
+        side = "periodic" if x["bc"] == 0 else "outflow"
+        c.boundary = mhd.MhdBoundarySpec([side] * 4, [side] * 4)
+        cfgs.append(c)
+    b = mhd.MhdBatch2D(cfgs)
+    for i, x in enumerate(insts):
+        for name, arr in zip(ics_components(), x["arrays"]()):
+            b.instance(i).seed_state(name, arr)
+    return b
+
+
+def ics_components():
+    from quasar_b200.ics import COMPONENTS
+    return COMPONENTS
+
+
 def seed(s, comps):
     from quasar_b200.ics import COMPONENTS
     for name, arr in zip(COMPONENTS, comps):
@@ -335,35 +359,45 @@ def main():
                    "div_b_max": s3.divergence_b_max()}
         del s3
 
-    # the batched plain step: 256 seeded independent MP5 instances on uneven
-    # grids, persistent per-phase launches in a CUDA graph, autotuned grids
-    batched = None
+    # batched steps: the 256-instance MP5 batch (plain), and the combined
+    # batch (OT 8192^2 MP7 + 64 rotor/blast instances) plain then learned
+    batched = combined = None
     if not a.no_batch:
-        from quasar_b200 import mhd as _mhd
-        insts = ics.batch_instances(count=256, seed=0, order=5)
-        cfgs = []
-        for x in insts:
-            c = _mhd.MhdConfig()
-            c.grid = _mhd.Grid2D(x["nx"], x["ny"], x["lx"], x["ly"])
-            c.reconstruction = "mp5"
-            c.gamma = x["gamma"]
-            side = "periodic" if x["bc"] == 0 else "outflow"
-            c.boundary = _mhd.MhdBoundarySpec([side] * 4, [side] * 4)
-            cfgs.append(c)
-        b = _mhd.MhdBatch2D(cfgs)
-        for i, x in enumerate(insts):
-            for name, arr in zip(ics.COMPONENTS, x["arrays"]()):
-                b.instance(i).seed_state(name, arr)
+        kb = max(10, a.steps // 10)
+        b = make_batch(ics.batch_instances(count=256, seed=0, order=5), 5)
         ctas, trials = b.autotune()
         b.time_steps(3)
-        bms, bzu = b.time_steps(max(10, a.steps // 10))
+        bms, bzu = b.time_steps(kb)
         bms = dist.reduce(bms, "max")
         batched = {"workload": "256 seeded MP5 instances, sides log-uniform in [64, 512], "
                                "Orszag-Tang / oblique Brio-Wu / linear fast or Alfven waves",
                    "zones": b.zones(), "value": bzu * WORLD / (bms * 1e-3), "unit": "zone-updates/s",
-                   "ms_per_step": bms / max(10, a.steps // 10), "autotuned_ctas_per_sm": ctas,
+                   "ms_per_step": bms / kb, "autotuned_ctas_per_sm": ctas,
                    "autotune_steps": trials}
         del b
+        if not a.no_learned:
+            from quasar_b200 import train_indicator
+            from quasar_b200.indicator import attach_batch
+            b = make_batch(ics.combined_instances(seed=2, order=7), 7)
+            ctas, trials = b.autotune()
+            b.time_steps(3)
+            pms, pzu = b.time_steps(kb)
+            ind, thr = train_indicator.load(order=7)
+            attach_batch(ind, b, thr)
+            b.time_steps(3)
+            lms, lzu = b.time_steps(kb)
+            pms, lms = dist.reduce(pms, "max"), dist.reduce(lms, "max")
+            combined = {"workload": "one batch: Orszag-Tang 8192^2 MP7 + 64 seeded rotor/blast MP7 "
+                                    "instances, sides log-uniform in [256, 1024]",
+                        "zones": b.zones(), "unit": "zone-updates/s",
+                        "plain_batched": pzu * WORLD / (pms * 1e-3),
+                        "learned_batched": lzu * WORLD / (lms * 1e-3),
+                        "speedup": (lzu / lms) / (pzu / pms),
+                        "ms_per_step_plain": pms / kb, "ms_per_step_learned": lms / kb,
+                        "note": "plain steps first, then the learned steps continue the same "
+                                "batch; the density L1 gap is measured by the `learned` line "
+                                "and tests/test_gpu_batch.py"}
+            del b
 
     cpu = None
     if RANK == 0 and WORLD == 1 and not a.no_cpu:
@@ -380,7 +414,7 @@ def main():
                            "l2": "state 1 GB+ per register, larger than L2"},
                 "gpu_launches": LAUNCHES_PER_STEP * a.steps,
                 "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
-                "learned": learned, "batched": batched}
+                "learned": learned, "batched": batched, "batched_learned": combined}
         print(json.dumps(line), flush=True)
     dist.close()
 

@@ -343,3 +343,23 @@ def _ot_field_scaled(n, order, scale):
     out[4] = np.ascontiguousarray(arr[4] - old_mag + 0.5 * (bx ** 2 + by ** 2))
     out[5], out[6] = np.ascontiguousarray(bx), np.ascontiguousarray(by)
     return out
+
+
+def combined_instances(seed=2, count=64, lo=256, hi=1024, order=7, ot_n=8192):
+    """The large combined batch: one Orszag-Tang instance at ot_n^2 and
+    `count` rotor / blast instances (alternating) with square sides
+    log-uniform in [lo, hi] and radii log-uniform in [0.05, 0.2], outflow.
+    Returns dicts like batch_instances."""
+    rng = np.random.default_rng(seed)
+    out = [dict(family="orszag_tang", nx=ot_n, ny=ot_n, lx=1.0, ly=1.0, gamma=5.0 / 3.0, bc=0,
+                arrays=lambda: orszag_tang(ot_n, order=order))]
+    for k in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        r0 = float(math.exp(rng.uniform(math.log(0.05), math.log(0.2))))
+        if k % 2 == 0:
+            out.append(dict(family="rotor", nx=n, ny=n, lx=1.0, ly=1.0, gamma=5.0 / 3.0, bc=1,
+                            radius=r0, arrays=lambda n=n, r0=r0: rotor(n, order=order, r0=r0)))
+        else:
+            out.append(dict(family="blast", nx=n, ny=n, lx=1.0, ly=1.0, gamma=5.0 / 3.0, bc=1,
+                            radius=r0, arrays=lambda n=n, r0=r0: blast(n, order=order, radius=r0)))
+    return out
