@@ -1020,32 +1020,63 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
 
 // ---------------------------------------------------------------------------
 // MP5/MP7 face flux with one lane per Gauss point: a group of four lanes owns
-// a face (eight faces per warp).  Each lane recovers its point state and
-// solves its Riemann problem; the group votes on admissibility, gathers the
-// point fluxes in node order for the Gauss sum, and splits the stores.
-// Same arithmetic as k_face_flux (node order of every sum kept).
+// a face.  Each lane recovers its point state and solves its Riemann problem;
+// the group votes on admissibility, gathers the point fluxes in node order for
+// the Gauss sum, and splits the stores.  Same arithmetic as k_face_flux (node
+// order of every sum kept).  The interface states of a 16 x 4 face tile and
+// its transverse halo are staged in shared memory, so each stencil row is
+// read from L2 once per tile instead of once per face row (2.8x fewer for x
+// faces, 5x for y faces at MP7).  256 threads: 64 faces x 4 Gauss lanes.
 // ---------------------------------------------------------------------------
 namespace {
 
+constexpr int kFqTX = 16, kFqTY = 4;
+
 template <int DIR, int ORDER>
-__device__ __forceinline__ void b_face_flux_q(const Grid& g, const IfaceP& in, const FluxP& out,
-                                              double* emf, int* nj, double* spd, double gamma,
-                                              const Ctl* ctl, int bx, int by) {
+__device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, const FluxP& out,
+                                               double* emf, int* nj, double* spd, double gamma,
+                                               const Ctl* ctl, int bx, int by) {
   constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
+  constexpr int TR = DIR == 0 ? kFqTY + 2 * H : kFqTY;   // tile rows (j)
+  constexpr int TC = DIR == 0 ? kFqTX : kFqTX + 2 * H;   // tile columns (i)
+  __shared__ double tile[16][TR][TC];
+  if (ctl->status) return;  // uniform over the block
+  const int i0 = bx * kFqTX, j0 = by * kFqTY;
+  const bool perx = g.bc[0] == 0 && g.bc[1] == 0, pery = g.bc[2] == 0 && g.bc[3] == 0;
+  for (int e = threadIdx.x; e < TR * TC; e += blockDim.x) {
+    const int row = e / TC, col = e - row * TC;
+    int fi, fj;
+    bool valid;
+    if (DIR == 0) {
+      const int ii = i0 + col;
+      fi = (ii == g.nx && perx) ? 0 : ii;
+      fj = j0 - H + row;
+      valid = ii <= g.nx && fj >= -g.ng && fj < g.ny + g.ng;
+    } else {
+      const int jj = j0 + row;
+      fj = (jj == g.ny && pery) ? 0 : jj;
+      fi = i0 - H + col;
+      valid = jj <= g.ny && fi >= -g.ng && fi < g.nx + g.ng;
+    }
+    const long long kk = valid ? g.idx(fi, fj) : 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      tile[c][row][col] = valid ? __ldg(in.L[c] + kk) : 0.0;
+      tile[8 + c][row][col] = valid ? __ldg(in.R[c] + kk) : 0.0;
+    }
+  }
+  __syncthreads();
   constexpr bool kLF = false;
-  const int lane = threadIdx.x & 3;
+  const int lane = threadIdx.x & 3, grp = threadIdx.x >> 2;
   const unsigned gmask = 0xFu << (threadIdx.x & 28);
-  const int i = bx * 32 + (threadIdx.x >> 2);
-  const int j = by;
+  const int fx = grp % kFqTX, fy = grp / kFqTX;
+  const int i = i0 + fx, j = j0 + fy;
   if (i > g.nx || j > g.ny) return;  // whole four-lane groups leave together
-  if (ctl->status) return;
-  int si = i, sj = j;
-  if (DIR == 0 && i == g.nx && g.bc[0] == 0 && g.bc[1] == 0) si = 0;
-  if (DIR == 1 && j == g.ny && g.bc[2] == 0 && g.bc[3] == 0) sj = 0;
-  const long long k = g.idx(i, j), ks = g.idx(si, sj);
+  const long long k = g.idx(i, j);
   const double h = DIR == 0 ? g.dx : g.dy;
-  const long long ts = DIR == 0 ? g.pitch : 1;
-  // this lane's Gauss node (lanes >= Q only help with the base problem)
+  // tile coordinates of stencil tap t (t = H is the face itself)
+  auto tr = [&](int t) { return DIR == 0 ? fy + t : fy; };
+  auto tcl = [&](int t) { return DIR == 0 ? fx : fx + t; };
   St l{}, r{};
   bool ok = true;
   if (lane < Q) {
@@ -1058,8 +1089,8 @@ __device__ __forceinline__ void b_face_flux_q(const Grid& g, const IfaceP& in, c
       double sa[N], sb[N];
 #pragma unroll
       for (int t = 0; t < N; ++t) {
-        sa[t] = __ldg(in.L[c] + ks + (t - H) * ts);
-        sb[t] = __ldg(in.R[c] + ks + (t - H) * ts);
+        sa[t] = tile[c][tr(t)][tcl(t)];
+        sb[t] = tile[8 + c][tr(t)][tcl(t)];
       }
       pl[c] = wsum<N>(w, sa);
       pr[c] = wsum<N>(w, sb);
@@ -1068,19 +1099,23 @@ __device__ __forceinline__ void b_face_flux_q(const Grid& g, const IfaceP& in, c
     r = St{pr[0], pr[1], pr[2], pr[3], pr[4], pr[5], pr[6], pr[7]};
     ok = point_admissible(l, gamma) && point_admissible(r, gamma);
   }
+  auto centre = [&](bool left) {
+    const int o = left ? 0 : 8, rr = tr(H), cc = tcl(H);
+    return St{tile[o][rr][cc],     tile[o + 1][rr][cc], tile[o + 2][rr][cc], tile[o + 3][rr][cc],
+              tile[o + 4][rr][cc], tile[o + 5][rr][cc], tile[o + 6][rr][cc], tile[o + 7][rr][cc]};
+  };
   const unsigned bad = (__ballot_sync(gmask, !ok) >> (threadIdx.x & 28)) & 0xFu;
   const bool group_ok = bad == 0;
   const int first_bad = bad ? __ffs(bad) - 1 : Q;
   double rate = 0.0;
   if (spd) {
-    if (lane == 0) rate = face_rate<DIR, ORDER>(iface(in, ks, true), iface(in, ks, false), gamma, h);
+    if (lane == 0) rate = face_rate<DIR, ORDER>(centre(true), centre(false), gamma, h);
     if (lane < first_bad) rate = fmax(rate, face_rate<DIR, ORDER>(l, r, gamma, h));
   }
-  // one Riemann solve per lane: its point, or (fallback) the face average
   const bool solve = group_ok ? lane < Q : lane == 0;
   if (!group_ok) {
-    l = iface(in, ks, true);
-    r = iface(in, ks, false);
+    l = centre(true);
+    r = centre(false);
   }
   double fv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (solve) {
@@ -1100,7 +1135,6 @@ __device__ __forceinline__ void b_face_flux_q(const Grid& g, const IfaceP& in, c
       res[c] = __shfl_sync(gmask, fv[c], 0, 4);
     }
   }
-  // stores split over the group: lane q writes components q and q+4
   const double lo = lane == 0 ? res[0] : lane == 1 ? res[1] : lane == 2 ? res[2] : res[3];
   const double hi = lane == 0 ? res[4] : lane == 1 ? res[5] : lane == 2 ? res[6] : res[7];
   double* const flo = lane == 0 ? out.f[0] : lane == 1 ? out.f[1] : lane == 2 ? out.f[2] : out.f[3];
@@ -1113,10 +1147,10 @@ __device__ __forceinline__ void b_face_flux_q(const Grid& g, const IfaceP& in, c
     rate = fmax(rate, __shfl_xor_sync(gmask, rate, 2, 4));
     if (lane == 0) spd[k] = rate;
   }
-  // no-jump proof over the 2H+1 transverse taps, split across the group
-  constexpr int RH = H;
+  // no-jump proof over the 2H+1 transverse taps (mapped like every CT table
+  // read), split across the group
   int proof = 1;
-  for (int off = lane - RH; off <= RH; off += 4) {
+  for (int off = lane - H; off <= H; off += 4) {
     const int mi = face_index(DIR == 0 ? i : i + off, g.nx, g.bc[0], g.bc[1]);
     const int mj = face_index(DIR == 0 ? j + off : j, g.ny, g.bc[2], g.bc[3]);
     if (!in_pad(g, mi, mj)) {
@@ -1133,10 +1167,10 @@ __device__ __forceinline__ void b_face_flux_q(const Grid& g, const IfaceP& in, c
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128, 4) k_face_flux_q(Grid g, IfaceP in, FluxP out, double* emf,
-                                                     int* nj, double* spd, double gamma,
-                                                     const Ctl* ctl) {
-  b_face_flux_q<DIR, ORDER>(g, in, out, emf, nj, spd, gamma, ctl, blockIdx.x, blockIdx.y);
+__global__ void __launch_bounds__(256, 2) k_face_flux_qs(Grid g, IfaceP in, FluxP out, double* emf,
+                                                         int* nj, double* spd, double gamma,
+                                                         const Ctl* ctl) {
+  b_face_flux_qs<DIR, ORDER>(g, in, out, emf, nj, spd, gamma, ctl, blockIdx.x, blockIdx.y);
 }
 
 }  // namespace
@@ -1776,16 +1810,17 @@ __global__ void kb_face_lists(const BatchRec* __restrict__ r, const BatchLearnRe
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128, 4) kb_face_flux_q(const BatchRec* __restrict__ r,
+__global__ void __launch_bounds__(256, 2) kb_face_flux_q(const BatchRec* __restrict__ r,
                                                          BatchPlan p, int speeds) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
     int local, bx, by;
     const BatchRec& q = r[batch_locate(p, t, &local)];
     batch_block(kBpFlux, q.a.g, local, &bx, &by);
-    b_face_flux_q<DIR, ORDER>(q.a.g, DIR == 0 ? q.a.ix : q.a.iy, DIR == 0 ? q.a.fx : q.a.fy,
-                              DIR == 0 ? q.a.xemf : q.a.yemf, DIR == 0 ? q.a.xnj : q.a.ynj,
-                              speeds ? (DIR == 0 ? q.a.xspd : q.a.yspd) : nullptr, q.a.gamma,
-                              q.a.ctl, bx, by);
+    b_face_flux_qs<DIR, ORDER>(q.a.g, DIR == 0 ? q.a.ix : q.a.iy, DIR == 0 ? q.a.fx : q.a.fy,
+                               DIR == 0 ? q.a.xemf : q.a.yemf, DIR == 0 ? q.a.xnj : q.a.ynj,
+                               speeds ? (DIR == 0 ? q.a.xspd : q.a.yspd) : nullptr, q.a.gamma,
+                               q.a.ctl, bx, by);
+    __syncthreads();  // the shared tile is reused by the next tile
   }
 }
 
@@ -1920,8 +1955,8 @@ template <int DIR, int ORDER>
 static void flux_launch(const StageArgs& a, bool speeds, cudaStream_t s) {
   const Grid& g = a.g;
   if (ORDER == 5 || ORDER == 7) {
-    const dim3 grid(cdiv(g.nx + 1, 32), g.ny + 1);
-    k_face_flux_q<DIR, ORDER == 5 ? 5 : 7><<<grid, 128, 0, s>>>(
+    const dim3 grid(cdiv(g.nx + 1, kFqTX), cdiv(g.ny + 1, kFqTY));
+    k_face_flux_qs<DIR, ORDER == 5 ? 5 : 7><<<grid, 256, 0, s>>>(
         g, DIR == 0 ? a.ix : a.iy, DIR == 0 ? a.fx : a.fy, DIR == 0 ? a.xemf : a.yemf,
         DIR == 0 ? a.xnj : a.ynj, speeds ? (DIR == 0 ? a.xspd : a.yspd) : nullptr, a.gamma, a.ctl);
     return;
@@ -2038,7 +2073,7 @@ void batch_cell_configure() {
 
 int batch_phase_threads(int phase) {
   switch (phase) {
-    case kBpRecon0: case kBpRecon1: case kBpFlux: case kBpCorner: return 128;
+    case kBpRecon0: case kBpRecon1: case kBpCorner: return 128;
     default: return 256;
   }
 }
@@ -2048,7 +2083,7 @@ int batch_phase_max_ctas_per_sm(int phase, int order) {
   switch (phase) {
     case kBpRecon0: return o7 ? max_ctas(kb_reconstruct<0, 7>, 128, 0) : max_ctas(kb_reconstruct<0, 5>, 128, 0);
     case kBpRecon1: return o7 ? max_ctas(kb_reconstruct<1, 7>, 128, 0) : max_ctas(kb_reconstruct<1, 5>, 128, 0);
-    case kBpFlux: return o7 ? max_ctas(kb_face_flux_q<0, 7>, 128, 0) : max_ctas(kb_face_flux_q<0, 5>, 128, 0);
+    case kBpFlux: return o7 ? max_ctas(kb_face_flux_q<0, 7>, 256, 0) : max_ctas(kb_face_flux_q<0, 5>, 256, 0);
     case kBpCell:
       if (o7) {
         batch_cell_configure<7>();
@@ -2079,11 +2114,11 @@ void launch_batch_face_flux(const BatchRec* r, const BatchPlan& p, int dir, int 
                             bool speeds, cudaStream_t s) {
   const int sp = speeds ? 1 : 0;
   if (order == 7) {
-    if (dir == 0) kb_face_flux_q<0, 7><<<pgrid(p), 128, 0, s>>>(r, p, sp);
-    else kb_face_flux_q<1, 7><<<pgrid(p), 128, 0, s>>>(r, p, sp);
+    if (dir == 0) kb_face_flux_q<0, 7><<<pgrid(p), 256, 0, s>>>(r, p, sp);
+    else kb_face_flux_q<1, 7><<<pgrid(p), 256, 0, s>>>(r, p, sp);
   } else {
-    if (dir == 0) kb_face_flux_q<0, 5><<<pgrid(p), 128, 0, s>>>(r, p, sp);
-    else kb_face_flux_q<1, 5><<<pgrid(p), 128, 0, s>>>(r, p, sp);
+    if (dir == 0) kb_face_flux_q<0, 5><<<pgrid(p), 256, 0, s>>>(r, p, sp);
+    else kb_face_flux_q<1, 5><<<pgrid(p), 256, 0, s>>>(r, p, sp);
   }
 }
 
