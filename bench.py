@@ -279,9 +279,10 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tpath):
         tt = json.load(open(tpath)).get(f"{a.case}_mp{a.order}_reconstruction")
-        if tt:
-            traffic = tt["bytes_per_zone_step"] * zones
-    roofline = {"bound": "fp64", "kernel": "k_reconstruct (x and y, 3 stages)",
+        if tt:  # DRAM bytes of one reconstruction launch (6 launches per step)
+            traffic = tt["bytes_per_zone_step"] / 6.0 * zones
+    roofline = {"bound": "fp64", "kernel": "k_reconstruct (x and y, 3 stages; achieved over "
+                                          "the phase, traffic per launch)",
                 "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                 "frac": (achieved / peak.value) if achieved else None, "traffic": traffic,
                 "peak_source": "FP64 FMA probe on this GPU (qmhd_fp64_fma_peak); "

@@ -20,6 +20,10 @@
 #include "mhd_device.cuh"
 #include "mhd_kernels.cuh"
 
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
 namespace qb {
 
 namespace {
@@ -489,14 +493,10 @@ __device__ __forceinline__ void conserved_row_col(const Eg& e, int k, double* Lr
   Rc[6] = rp[6];
 }
 
-__device__ __forceinline__ void conserved_row(const Eg& e, int k, double* Lr) {
-  double Rc[7];
-  conserved_row_col(e, k, Lr, Rc);
-}
-__device__ __forceinline__ void conserved_col(const Eg& e, int k, double* Rc) {
-  double Lr[7];
-  conserved_row_col(e, k, Lr, Rc);
-}
+// Dynamic shared memory of every kernel that runs mp_pair_loop: 98 doubles
+// (7 L rows + 7 R columns) per thread of a 128-thread block.
+constexpr int kReconThreads = 128;
+constexpr size_t kReconSmem = 98 * kReconThreads * sizeof(double);
 
 template <int DIR, int H>
 __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, double gamma, St& ul,
@@ -514,29 +514,49 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
   ref.bz = 0.5 * cl.bz + 0.5 * cr.bz;
   const St c = rot<DIR>(ref);
   const Eg e = eig_scalars(c, gamma);
-  // L R = I check (mhd_eigensystem.hpp:416-430), R columns resident in two
-  // halves (4 + 3) against L rows rebuilt one at a time
+  // All seven L rows and R columns built once into this thread's slots of
+  // dynamic shared memory (kReconSmemDoubles per thread, stride = threads per
+  // block), then the L R = I check (mhd_eigensystem.hpp:416-430) with R
+  // resident in two halves (4 + 3).  |d| <= 1024 eps is tested as
+  // d^2 <= (1024 eps)^2, the same decision since 1024 eps is a power of two
+  // (and false for NaN and infinity).
+  extern __shared__ double dsm[];
+  const int ST = blockDim.x * blockDim.y;
+  double* LR = dsm + (threadIdx.y * blockDim.x + threadIdx.x);
+#pragma unroll 1
+  for (int k = 0; k < 7; ++k) {
+    double Lr[7], Rc[7];
+    conserved_row_col(e, k, Lr, Rc);
+#pragma unroll
+    for (int m = 0; m < 7; ++m) {
+      LR[(k * 7 + m) * ST] = Lr[m];
+      LR[(49 + k * 7 + m) * ST] = Rc[m];
+    }
+  }
   bool usable = true;
+  constexpr double kT2 = (1024.0 * kEps) * (1024.0 * kEps);
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
     constexpr int kCols = 4;
     const int j0 = half * kCols, nj = half == 0 ? kCols : 7 - kCols;
-    double R[kCols][7];
+    double Rm[kCols][7];
 #pragma unroll
     for (int jj = 0; jj < kCols; ++jj)
-      if (jj < nj) conserved_col(e, j0 + jj, R[jj]);
+#pragma unroll
+      for (int m = 0; m < 7; ++m) Rm[jj][m] = jj < nj ? LR[(49 + (j0 + jj) * 7 + m) * ST] : 0.0;
 #pragma unroll 1
     for (int i = 0; i < 7; ++i) {
       double Lr[7];
-      conserved_row(e, i, Lr);
+#pragma unroll
+      for (int m = 0; m < 7; ++m) Lr[m] = LR[(i * 7 + m) * ST];
 #pragma unroll
       for (int jj = 0; jj < kCols; ++jj) {
         if (jj >= nj) continue;
         double dot = 0.0;
 #pragma unroll
-        for (int m = 0; m < 7; ++m) dot += Lr[m] * R[jj][m];
-        const double expect = i == j0 + jj ? 1.0 : 0.0;
-        if (!isfinite(dot) || fabs(dot - expect) > 1024.0 * kEps) usable = false;
+        for (int m = 0; m < 7; ++m) dot += Lr[m] * Rm[jj][m];
+        const double d = dot - (i == j0 + jj ? 1.0 : 0.0);
+        usable = usable && (d * d <= kT2);
       }
     }
   }
@@ -563,7 +583,8 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
   for (int k = 0; k < 7; ++k) {
     double Lr[7];
     if (usable) {
-      conserved_row(e, k, Lr);
+#pragma unroll
+      for (int m = 0; m < 7; ++m) Lr[m] = LR[(k * 7 + m) * ST];
     } else {
 #pragma unroll
       for (int v = 0; v < 7; ++v) Lr[v] = v == k ? 1.0 : 0.0;
@@ -586,7 +607,8 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
     const double wr = mp_recon<W>(win, f);
     double Rc[7];
     if (usable) {
-      conserved_col(e, k, Rc);
+#pragma unroll
+      for (int m = 0; m < 7; ++m) Rc[m] = LR[(49 + k * 7 + m) * ST];
     } else {
 #pragma unroll
       for (int v = 0; v < 7; ++v) Rc[v] = v == k ? 1.0 : 0.0;
@@ -728,7 +750,7 @@ __device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const
     muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
   } else {
     constexpr int H = ORDER == 5 ? 2 : 3;
-    if (MODE == 2) {
+    if constexpr (MODE == 2) {
       mp_pair_lin<DIR, H>(u, k0, step, ul, ur);
     } else {
       mp_pair_loop<DIR, H>(u, k0, step, gamma, ul, ur);
@@ -1377,7 +1399,7 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(256) k_cell_emf_s(Grid g, StateP u, double* cell_ez,
+__global__ void __launch_bounds__(256, 3) k_cell_emf_s(Grid g, StateP u, double* cell_ez,
                                                     const double* xs, const double* ys,
                                                     int cfl_reduce, double gamma, Ctl* ctl) {
   b_cell_emf_s<ORDER>(g, u, cell_ez, xs, ys, cfl_reduce, gamma, ctl, blockIdx.x, blockIdx.y);
@@ -1825,7 +1847,7 @@ __global__ void __launch_bounds__(256, 2) kb_face_flux_q(const BatchRec* __restr
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(256) kb_cell_emf_s(const BatchRec* __restrict__ r, BatchPlan p,
+__global__ void __launch_bounds__(256, 3) kb_cell_emf_s(const BatchRec* __restrict__ r, BatchPlan p,
                                                      int cfl_reduce) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
     int local, bx, by;
@@ -1901,6 +1923,16 @@ __global__ void kb_ctl(const BatchRec* __restrict__ r, int n, int what, double t
 // ===========================================================================
 namespace {
 inline unsigned cdiv(long long a, int b) { return unsigned((a + b - 1) / b); }
+
+// Raise a kernel's dynamic shared-memory limit once (per process).
+void ensure_smem(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::vector<const void*> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (std::find(done.begin(), done.end(), fn) != done.end()) return;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  done.push_back(fn);
+}
 }  // namespace
 
 void launch_fill_ghosts(const Grid& g, const StateP& u, cudaStream_t s) {
@@ -1940,7 +1972,13 @@ static void recon_launch(const StageArgs& a, cudaStream_t s) {
   const int ni = DIR == 0 ? g.nx + 1 : g.nx + 2 * g.ng;
   const int nj = DIR == 0 ? g.ny + 2 * g.ng : g.ny + 1;
   const dim3 grid(cdiv(ni, kBX), cdiv(nj, 4));
-  k_reconstruct<DIR, ORDER><<<grid, block, 0, s>>>(g, a.u, DIR == 0 ? a.ix : a.iy, a.gamma, a.ctl);
+  size_t smem = 0;
+  if (ORDER == 5 || ORDER == 7) {
+    smem = kReconSmem;
+    ensure_smem((const void*)k_reconstruct<DIR, ORDER>, smem);
+  }
+  k_reconstruct<DIR, ORDER><<<grid, block, smem, s>>>(g, a.u, DIR == 0 ? a.ix : a.iy, a.gamma,
+                                                      a.ctl);
 }
 
 void launch_reconstruct(const StageArgs& a, int dir, cudaStream_t s) {
@@ -2081,8 +2119,16 @@ int batch_phase_threads(int phase) {
 int batch_phase_max_ctas_per_sm(int phase, int order) {
   const bool o7 = order == 7;
   switch (phase) {
-    case kBpRecon0: return o7 ? max_ctas(kb_reconstruct<0, 7>, 128, 0) : max_ctas(kb_reconstruct<0, 5>, 128, 0);
-    case kBpRecon1: return o7 ? max_ctas(kb_reconstruct<1, 7>, 128, 0) : max_ctas(kb_reconstruct<1, 5>, 128, 0);
+    case kBpRecon0:
+      ensure_smem((const void*)kb_reconstruct<0, 7>, kReconSmem);
+      ensure_smem((const void*)kb_reconstruct<0, 5>, kReconSmem);
+      return o7 ? max_ctas(kb_reconstruct<0, 7>, 128, kReconSmem)
+                : max_ctas(kb_reconstruct<0, 5>, 128, kReconSmem);
+    case kBpRecon1:
+      ensure_smem((const void*)kb_reconstruct<1, 7>, kReconSmem);
+      ensure_smem((const void*)kb_reconstruct<1, 5>, kReconSmem);
+      return o7 ? max_ctas(kb_reconstruct<1, 7>, 128, kReconSmem)
+                : max_ctas(kb_reconstruct<1, 5>, 128, kReconSmem);
     case kBpFlux: return o7 ? max_ctas(kb_face_flux_q<0, 7>, 256, 0) : max_ctas(kb_face_flux_q<0, 5>, 256, 0);
     case kBpCell:
       if (o7) {
@@ -2102,11 +2148,21 @@ void launch_batch_reconstruct(const BatchRec* r, const BatchPlan& p, int dir, in
                               cudaStream_t s) {
   const dim3 block(32, 4);
   if (order == 7) {
-    if (dir == 0) kb_reconstruct<0, 7><<<pgrid(p), block, 0, s>>>(r, p);
-    else kb_reconstruct<1, 7><<<pgrid(p), block, 0, s>>>(r, p);
+    if (dir == 0) {
+      ensure_smem((const void*)kb_reconstruct<0, 7>, kReconSmem);
+      kb_reconstruct<0, 7><<<pgrid(p), block, kReconSmem, s>>>(r, p);
+    } else {
+      ensure_smem((const void*)kb_reconstruct<1, 7>, kReconSmem);
+      kb_reconstruct<1, 7><<<pgrid(p), block, kReconSmem, s>>>(r, p);
+    }
   } else {
-    if (dir == 0) kb_reconstruct<0, 5><<<pgrid(p), block, 0, s>>>(r, p);
-    else kb_reconstruct<1, 5><<<pgrid(p), block, 0, s>>>(r, p);
+    if (dir == 0) {
+      ensure_smem((const void*)kb_reconstruct<0, 5>, kReconSmem);
+      kb_reconstruct<0, 5><<<pgrid(p), block, kReconSmem, s>>>(r, p);
+    } else {
+      ensure_smem((const void*)kb_reconstruct<1, 5>, kReconSmem);
+      kb_reconstruct<1, 5><<<pgrid(p), block, kReconSmem, s>>>(r, p);
+    }
   }
 }
 
@@ -2174,18 +2230,22 @@ void launch_batch_reconstruct_learned(const BatchRec* r, const BatchLearnRec* l,
   if (order == 7) {
     if (dir == 0) {
       kb_reconstruct<0, 7, 2><<<pgrid(p), block, 0, s>>>(r, p);
-      kb_reconstruct_list<0, 7><<<list_grid, 128, 0, s>>>(r, l, p.n);
+      ensure_smem((const void*)kb_reconstruct_list<0, 7>, kReconSmem);
+      kb_reconstruct_list<0, 7><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
     } else {
       kb_reconstruct<1, 7, 2><<<pgrid(p), block, 0, s>>>(r, p);
-      kb_reconstruct_list<1, 7><<<list_grid, 128, 0, s>>>(r, l, p.n);
+      ensure_smem((const void*)kb_reconstruct_list<1, 7>, kReconSmem);
+      kb_reconstruct_list<1, 7><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
     }
   } else {
     if (dir == 0) {
       kb_reconstruct<0, 5, 2><<<pgrid(p), block, 0, s>>>(r, p);
-      kb_reconstruct_list<0, 5><<<list_grid, 128, 0, s>>>(r, l, p.n);
+      ensure_smem((const void*)kb_reconstruct_list<0, 5>, kReconSmem);
+      kb_reconstruct_list<0, 5><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
     } else {
       kb_reconstruct<1, 5, 2><<<pgrid(p), block, 0, s>>>(r, p);
-      kb_reconstruct_list<1, 5><<<list_grid, 128, 0, s>>>(r, l, p.n);
+      ensure_smem((const void*)kb_reconstruct_list<1, 5>, kReconSmem);
+      kb_reconstruct_list<1, 5><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
     }
   }
 }
@@ -2209,7 +2269,8 @@ void launch_reconstruct_label(const StageArgs& a, int dir, int* label, cudaStrea
   const IfaceP out = dir == 0 ? a.ix : a.iy;
 #define QB_LBL(D, O)                                                                          \
   if (dir == D && a.order == O)                                                              \
-    return (void)k_reconstruct_label<D, O><<<recon_grid<D, O>(a.g), block, 0, s>>>(         \
+    ensure_smem((const void*)k_reconstruct_label<D, O>, kReconSmem);                          \
+    return (void)k_reconstruct_label<D, O><<<recon_grid<D, O>(a.g), block, kReconSmem, s>>>( \
         a.g, a.u, out, a.gamma, a.ctl, label);
   QB_LBL(0, 5) QB_LBL(1, 5) QB_LBL(0, 7) QB_LBL(1, 7)
 #undef QB_LBL
@@ -2223,7 +2284,9 @@ void launch_reconstruct_learned(const StageArgs& a, int dir, const int* list, co
   if (dir == D && a.order == O) {                                                            \
     k_reconstruct_lin<D, O><<<recon_grid<D, O>(a.g), block, 0, s>>>(a.g, a.u, out, a.gamma,  \
                                                                     a.ctl);                  \
-    k_reconstruct_list<D, O><<<list_grid, 128, 0, s>>>(a.g, a.u, out, a.gamma, a.ctl, list,   \
+    ensure_smem((const void*)k_reconstruct_list<D, O>, kReconSmem);                           \
+    k_reconstruct_list<D, O><<<list_grid, 128, kReconSmem, s>>>(a.g, a.u, out, a.gamma, a.ctl, \
+                                                                list,                         \
                                                        count);                               \
     return;                                                                                  \
   }
