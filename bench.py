@@ -41,10 +41,21 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 WORLD = int(os.environ.get("WORLD_SIZE", "1"))
 RANK = int(os.environ.get("RANK", "0"))
 LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
-if WORLD > 1 and "CUDA_VISIBLE_DEVICES" not in os.environ:
-    # the solver library carries its own CUDA runtime: pin the device before
-    # any CUDA initialisation in this process
-    os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+
+def pin_rank_device(env, local_rank):
+    """One GPU per rank: the solver library carries its own CUDA runtime and
+    uses device 0 of what it sees, so narrow CUDA_VISIBLE_DEVICES to this
+    rank's GPU (the local_rank-th listed one, or local_rank itself when the
+    variable is unset) before any CUDA initialisation in this process."""
+    listed = [d for d in env.get("CUDA_VISIBLE_DEVICES", "").split(",") if d.strip()]
+    if "CUDA_VISIBLE_DEVICES" not in env:
+        env["CUDA_VISIBLE_DEVICES"] = str(local_rank)
+    elif local_rank < len(listed):
+        env["CUDA_VISIBLE_DEVICES"] = listed[local_rank].strip()
+
+
+if WORLD > 1:
+    pin_rank_device(os.environ, LOCAL_RANK)
 sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
