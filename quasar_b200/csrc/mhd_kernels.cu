@@ -20,11 +20,16 @@
 #include "mhd_device.cuh"
 #include "mhd_kernels.cuh"
 
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
 #include <algorithm>
 #include <mutex>
 #include <vector>
 
 namespace qb {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -243,6 +248,16 @@ __device__ __forceinline__ unsigned long long dbits(double x) {
   return (unsigned long long)__double_as_longlong(x);
 }
 
+// atomicMax of non-negative double bit patterns, one atomic per group of
+// converged lanes: the per-cell maxima of a developed flow hit one address
+// from nearly every cell, and same-address atomics serialise in L2.  The max
+// is exact and order-free, so the stored value is the per-cell one's.
+__device__ __forceinline__ void atomic_max_lanes(unsigned long long* dst, unsigned long long v) {
+  const cg::coalesced_group grp = cg::coalesced_threads();
+  const unsigned long long m = cg::reduce(grp, v, cg::greater<unsigned long long>());
+  if (grp.thread_rank() == 0 && m != 0ull) atomicMax(dst, m);
+}
+
 // ulp of a finite double as used by the solenoidality preflight
 // (numerics/mhd_background_metrics.hpp:105-121).
 __device__ __forceinline__ double ulp_of(double x) {
@@ -316,12 +331,9 @@ __device__ __forceinline__ void b_colloc_check(const Grid& g, const StateP& cand
                   fabs(res) <= 0.5 * scale && fabs(res) <= 1024.0 * unc;
     }
     const double r = explained ? 0.0 : fabs(res);
-    if (!isfinite(r) || !isfinite(scale)) {
-      atomicMax(&ctl->divb_res, dbits(kInf));
-    } else {
-      if (r > 0.0) atomicMax(&ctl->divb_res, dbits(r));
-      if (scale > 0.0) atomicMax(&ctl->divb_scale, dbits(scale));
-    }
+    const bool finite = isfinite(r) && isfinite(scale);
+    atomic_max_lanes(&ctl->divb_res, !finite ? dbits(kInf) : r > 0.0 ? dbits(r) : 0ull);
+    atomic_max_lanes(&ctl->divb_scale, finite && scale > 0.0 ? dbits(scale) : 0ull);
   }
 }
 
@@ -1712,7 +1724,7 @@ __global__ void k_divb_linf(Grid g, StateP u, unsigned long long* out) {
                              __dadd_rn(__ddiv_rn(u.c[6][k + g.pitch], g.dy),
                                        __ddiv_rn(-u.c[6][k], g.dy)));
   const double v = isfinite(d) ? fabs(d) : kInf;
-  if (v > 0.0) atomicMax(out, dbits(v));
+  atomic_max_lanes(out, v > 0.0 ? dbits(v) : 0ull);
 }
 
 // Per-block compensated partial sums of rho and energy over the cells.
