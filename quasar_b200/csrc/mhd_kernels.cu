@@ -1074,6 +1074,7 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
   constexpr int TR = DIR == 0 ? kFqTY + 2 * H : kFqTY;   // tile rows (j)
   constexpr int TC = DIR == 0 ? kFqTX : kFqTX + 2 * H;   // tile columns (i)
   __shared__ double tile[16][TR][TC];
+  __shared__ unsigned char same[TR][TC];  // staged and L == R in every component
   if (ctl->status) return;  // uniform over the block
   const int i0 = bx * kFqTX, j0 = by * kFqTY;
   const bool perx = g.bc[0] == 0 && g.bc[1] == 0, pery = g.bc[2] == 0 && g.bc[3] == 0;
@@ -1093,11 +1094,16 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
       valid = jj <= g.ny && fi >= -g.ng && fi < g.nx + g.ng;
     }
     const long long kk = valid ? g.idx(fi, fj) : 0;
+    bool eq = valid;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      tile[c][row][col] = valid ? __ldg(in.L[c] + kk) : 0.0;
-      tile[8 + c][row][col] = valid ? __ldg(in.R[c] + kk) : 0.0;
+      const double a = valid ? __ldg(in.L[c] + kk) : 0.0;
+      const double b = valid ? __ldg(in.R[c] + kk) : 0.0;
+      tile[c][row][col] = a;
+      tile[8 + c][row][col] = b;
+      eq = eq && a == b;
     }
+    same[row][col] = eq;
   }
   __syncthreads();
   constexpr bool kLF = false;
@@ -1182,11 +1188,18 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
     if (lane == 0) spd[k] = rate;
   }
   // no-jump proof over the 2H+1 transverse taps (mapped like every CT table
-  // read), split across the group
+  // read), split across the group.  A tap whose mapped face is the one staged
+  // in its tile slot reads the staged comparison; the others read memory.
   int proof = 1;
   for (int off = lane - H; off <= H; off += 4) {
     const int mi = face_index(DIR == 0 ? i : i + off, g.nx, g.bc[0], g.bc[1]);
     const int mj = face_index(DIR == 0 ? j + off : j, g.ny, g.bc[2], g.bc[3]);
+    const int ti = DIR == 0 ? ((i == g.nx && perx) ? 0 : i) : i + off;
+    const int tj = DIR == 0 ? j + off : ((j == g.ny && pery) ? 0 : j);
+    if (mi == ti && mj == tj) {
+      if (!same[tr(off + H)][tcl(off + H)]) proof = 0;
+      continue;
+    }
     if (!in_pad(g, mi, mj)) {
       proof = 0;
       break;
