@@ -36,6 +36,15 @@ INDICATOR_EXPORTS = ("qmhd_indicator_create", "qmhd_indicator_destroy", "qmhd_in
                      "qmhd_indicator_threshold_for_recall", "qmhd_solver_set_indicator",
                      "qmhd_solver_learned_face_counts", "qmhd_batch_set_indicator")
 
+LAUNCH_EXPORTS = ("qmhd_launch_reconstruct", "qmhd_launch_hlld_flux", "qmhd_launch_flux_difference",
+                  "qmhd_launch_ct_emf_prepare", "qmhd_launch_ct_emf_finish",
+                  "qmhd_launch_emf_curl_rate", "qmhd_launch_rk_stage",
+                  "qmhd_launch_admissible_fraction", "qmhd_launch_cfl_max_rate",
+                  "qmhd_launch_ct_divb_linf", "qmhd_launch_ct_divb_relative_linf",
+                  "qmhd_launch_fill_ghosts_fluid", "qmhd_launch_fill_ghosts_field",
+                  "qmhd_launch_collocate_face_to_cell", "qmhd_launch_conserved_cell_sums")
+LAUNCH_SCRATCH_BYTES = 64
+
 
 class QmhdConfig(ctypes.Structure):
     _fields_ = [
@@ -116,6 +125,8 @@ def lib() -> ctypes.CDLL:
     L.qmhd_solver_set_indicator.argtypes = [vp, vp, ctypes.c_float]
     L.qmhd_batch_set_indicator.argtypes = [vp, vp, ctypes.c_float]
     L.qmhd_solver_learned_face_counts.argtypes = [vp, lp, lp]
+    from . import launch as _launch
+    _launch.declare(L)
     _lib = L
     return L
 

@@ -21,7 +21,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libquasar_mhd_b200.so")
-SOURCES = ["mhd_kernels.cu", "mhd_solver.cu", "mhd_batch.cu", "capi.cu", "probe.cu", "noalloc.cu", "indicator.cu"]
+SOURCES = ["mhd_kernels.cu", "mhd_solver.cu", "mhd_batch.cu", "capi.cu", "probe.cu", "noalloc.cu", "indicator.cu", "launch_abi.cu"]
 HEADERS = ["mhd_device.cuh", "mhd_kernels.cuh", "mhd_solver.cuh", "mhd_batch.cuh", "noalloc.cuh", "indicator.cuh", "tc.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -44,6 +44,7 @@ def _compile(src: str, force: bool, verbose: bool) -> str:
     deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS]
     deps.append(os.path.join(ROOT, "include", "quasar_mhd.h"))
     deps.append(os.path.join(ROOT, "include", "quasar_mhd_ext.h"))
+    deps.append(os.path.join(ROOT, "include", "quasar_mhd_launch.h"))
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= _newest(deps):
         return obj
     cmd = [nvcc(), *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]

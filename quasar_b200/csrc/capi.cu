@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -100,6 +101,12 @@ qb::Config to_config(const qmhd_config& q) {
 }
 
 }  // namespace
+
+namespace qb {
+// Status code and thread-local message of f() under the C ABI's rules; the
+// per-kernel launch interface (launch_abi.cu) reports through it.
+int capi_guarded(const std::function<void()>& f) { return guarded(f); }
+}  // namespace qb
 
 extern "C" {
 

@@ -144,35 +144,29 @@ __device__ __forceinline__ void ghost_src(int n, int layer, bool lo, int mode, i
   else si = lo ? layer - 1 : n - layer;
 }
 
-// axis 0: the x sides (both), all padded rows; axis 1: the y sides over all
-// padded columns (run after axis 0 so the corner blocks close last).
-__device__ __forceinline__ void b_fill_ghosts(const Grid& g, const StateP& u, int axis, int bx) {
-  const int lines = (axis == 0 ? g.ny : g.nx) + 2 * g.ng;
-  const int t = bx * blockDim.x + threadIdx.x;
-  if (t >= 2 * g.ng * lines) return;
-  const int side = t / (g.ng * lines);
-  const int rem = t - side * g.ng * lines;
-  const int layer = rem / lines + 1;
-  const int line = rem % lines - g.ng;
-  const bool lo = side == 0;
-  const int mode = g.bc[axis * 2 + side];
+// One ghost layer of one boundary line.  parts: bit 0 the fluid components
+// (rho, momentum, energy, bz_cell; a wall flips the normal momentum), bit 1
+// the staggered field (tangential face even; the normal face by its own rule).
+__device__ __forceinline__ void fill_ghost(const Grid& g, const StateP& u, int axis, bool lo,
+                                           int mode, int layer, int line, int parts) {
   const int n = axis == 0 ? g.nx : g.ny;
   int gi, si;
   ghost_src(n, layer, lo, mode, gi, si);
   auto at = [&](int a) { return axis == 0 ? g.idx(a, line) : g.idx(line, a); };
   const long long kd = at(gi), ks = at(si);
   const double sn = mode == 2 ? -1.0 : 1.0;
-  // fluid: the wall flips only the normal momentum
-  u.c[0][kd] = u.c[0][ks];
-  u.c[1][kd] = (axis == 0 ? sn : 1.0) * u.c[1][ks];
-  u.c[2][kd] = (axis == 1 ? sn : 1.0) * u.c[2][ks];
-  u.c[3][kd] = u.c[3][ks];
-  u.c[4][kd] = u.c[4][ks];
-  // field: tangential face and bz even; the normal face follows its own rule
+  if (parts & 1) {
+    u.c[0][kd] = u.c[0][ks];
+    u.c[1][kd] = (axis == 0 ? sn : 1.0) * u.c[1][ks];
+    u.c[2][kd] = (axis == 1 ? sn : 1.0) * u.c[2][ks];
+    u.c[3][kd] = u.c[3][ks];
+    u.c[4][kd] = u.c[4][ks];
+    u.c[7][kd] = u.c[7][ks];
+  }
+  if (!(parts & 2)) return;
   double* bn = axis == 0 ? u.c[5] : u.c[6];
   double* bt = axis == 0 ? u.c[6] : u.c[5];
   bt[kd] = bt[ks];
-  u.c[7][kd] = u.c[7][ks];
   if (mode == 2) {
     if (lo) {
       bn[at(0)] = 0.0;
@@ -188,6 +182,17 @@ __device__ __forceinline__ void b_fill_ghosts(const Grid& g, const StateP& u, in
   } else {
     bn[kd] = sn * bn[ks];
   }
+}
+
+// axis 0: the x sides (both), all padded rows; axis 1: the y sides over all
+// padded columns (run after axis 0 so the corner blocks close last).
+__device__ __forceinline__ void b_fill_ghosts(const Grid& g, const StateP& u, int axis, int bx) {
+  const int lines = (axis == 0 ? g.ny : g.nx) + 2 * g.ng;
+  const int t = bx * blockDim.x + threadIdx.x;
+  if (t >= 2 * g.ng * lines) return;
+  const int side = t / (g.ng * lines);
+  const int rem = t - side * g.ng * lines;
+  fill_ghost(g, u, axis, side == 0, g.bc[axis * 2 + side], rem / lines + 1, rem % lines - g.ng, 3);
 }
 
 __global__ void k_fill_ghosts(Grid g, StateP u, int axis) {
@@ -269,6 +274,35 @@ __device__ __forceinline__ double ulp_of(double x) {
   return ldexp(0.5, e - 52);
 }
 
+// Discrete div B of interior cell k relative to the directional scale
+// (mhd_reduce.hip:556-700, solver mhd_solver.cpp:1196-1222): the residual
+// the rounding envelope does not explain and the scale |d1| + |d2|, as bit
+// patterns of non-negative doubles (0 = nothing to record; a non-finite
+// stencil records an infinite residual).
+__device__ __forceinline__ void divb_cell(const Grid& g, const StateP& u, long long k,
+                                          int solver_owned, unsigned long long& rb,
+                                          unsigned long long& sb) {
+  const double bxl = u.c[5][k], bxh = u.c[5][k + 1];
+  const double byl = u.c[6][k], byh = u.c[6][k + g.pitch];
+  const double d1 = __ddiv_rn(__dadd_rn(bxh, -bxl), g.dx);
+  const double d2 = __ddiv_rn(__dadd_rn(byh, -byl), g.dy);
+  const double res = __dadd_rn(d1, d2);
+  const double scale = __dadd_rn(fabs(d1), fabs(d2));
+  const double unc = __dadd_rn(__ddiv_rn(__dadd_rn(ulp_of(bxh), ulp_of(bxl)), g.dx),
+                               __ddiv_rn(__dadd_rn(ulp_of(byh), ulp_of(byl)), g.dy));
+  bool explained;
+  if (solver_owned) {
+    explained = fabs(res) <= 1024.0 * unc;
+  } else {
+    explained = d1 != 0.0 && d2 != 0.0 && (signbit(d1) != signbit(d2)) &&
+                fabs(res) <= 0.5 * scale && fabs(res) <= 1024.0 * unc;
+  }
+  const double r = explained ? 0.0 : fabs(res);
+  const bool finite = isfinite(r) && isfinite(scale);
+  rb = !finite ? dbits(kInf) : r > 0.0 ? dbits(r) : 0ull;
+  sb = finite && scale > 0.0 ? dbits(scale) : 0ull;
+}
+
 // Collocate the candidate state's in-plane field (padded range) and, for
 // interior cells, run the admissibility fraction against `base` and the
 // live-state preflights.  theta_mask: bit0 collocation order 0, bit1 order 1,
@@ -313,27 +347,10 @@ __device__ __forceinline__ void b_colloc_check(const Grid& g, const StateP& cand
     const St b1 = load_cell1(cand, g, i, j);
     const double t1 = admissible_fraction(b1, b1);
     if (!(t1 >= 1.0)) atomicMin(&ctl->anchor_theta, dbits(t1));
-    // discrete div B relative to the directional scale
-    // (mhd_reduce.hip:556-700, solver mhd_solver.cpp:1196-1222)
-    const double bxl = cand.c[5][k], bxh = cand.c[5][k + 1];
-    const double byl = cand.c[6][k], byh = cand.c[6][k + g.pitch];
-    const double d1 = __ddiv_rn(__dadd_rn(bxh, -bxl), g.dx);
-    const double d2 = __ddiv_rn(__dadd_rn(byh, -byl), g.dy);
-    const double res = __dadd_rn(d1, d2);
-    const double scale = __dadd_rn(fabs(d1), fabs(d2));
-    const double unc = __dadd_rn(__ddiv_rn(__dadd_rn(ulp_of(bxh), ulp_of(bxl)), g.dx),
-                                 __ddiv_rn(__dadd_rn(ulp_of(byh), ulp_of(byl)), g.dy));
-    bool explained;
-    if (solver_owned) {
-      explained = fabs(res) <= 1024.0 * unc;
-    } else {
-      explained = d1 != 0.0 && d2 != 0.0 && (signbit(d1) != signbit(d2)) &&
-                  fabs(res) <= 0.5 * scale && fabs(res) <= 1024.0 * unc;
-    }
-    const double r = explained ? 0.0 : fabs(res);
-    const bool finite = isfinite(r) && isfinite(scale);
-    atomic_max_lanes(&ctl->divb_res, !finite ? dbits(kInf) : r > 0.0 ? dbits(r) : 0ull);
-    atomic_max_lanes(&ctl->divb_scale, finite && scale > 0.0 ? dbits(scale) : 0ull);
+    unsigned long long rb, sb;
+    divb_cell(g, cand, k, solver_owned, rb, sb);
+    atomic_max_lanes(&ctl->divb_res, rb);
+    atomic_max_lanes(&ctl->divb_scale, sb);
   }
 }
 
@@ -1020,17 +1037,22 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
       f.bz = gauss_avg<ORDER>(fq[7]);
     }
   }
-  out.f[0][k] = f.rho;
-  out.f[1][k] = f.mx;
-  out.f[2][k] = f.my;
-  out.f[3][k] = f.mz;
-  out.f[4][k] = f.E;
-  out.f[5][k] = f.bx;
-  out.f[6][k] = f.by;
-  out.f[7][k] = f.bz;
+  // out, emf and nj may each be absent (the per-kernel launch interface
+  // asks for fluxes or for the CT face tables alone)
+  if (out.f[0]) {
+    out.f[0][k] = f.rho;
+    out.f[1][k] = f.mx;
+    out.f[2][k] = f.my;
+    out.f[3][k] = f.mz;
+    out.f[4][k] = f.E;
+    out.f[5][k] = f.bx;
+    out.f[6][k] = f.by;
+    out.f[7][k] = f.bz;
+  }
   // Directional Godunov E_z: F_x(By) = -Ez, F_y(Bx) = +Ez (mhd_ct.hip:126-133).
-  emf[k] = DIR == 0 ? -f.by : f.bx;
+  if (emf) emf[k] = DIR == 0 ? -f.by : f.bx;
   if (spd) spd[k] = rate;
+  if (!nj) return;
   // "No jump" proof of the complete point-recovered problem
   // (mhd_ct.hip:150-174); taps are mapped like every CT table read.
   constexpr int RH = ORDER >= 7 ? 3 : ORDER >= 5 ? 2 : 0;
@@ -1179,14 +1201,19 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
   const double hi = lane == 0 ? res[4] : lane == 1 ? res[5] : lane == 2 ? res[6] : res[7];
   double* const flo = lane == 0 ? out.f[0] : lane == 1 ? out.f[1] : lane == 2 ? out.f[2] : out.f[3];
   double* const fhi = lane == 0 ? out.f[4] : lane == 1 ? out.f[5] : lane == 2 ? out.f[6] : out.f[7];
-  flo[k] = lo;
-  fhi[k] = hi;
-  if (lane == 0) emf[k] = DIR == 0 ? -res[6] : res[5];
+  // out, emf and nj may each be absent (the per-kernel launch interface
+  // asks for fluxes or for the CT face tables alone)
+  if (out.f[0]) {
+    flo[k] = lo;
+    fhi[k] = hi;
+  }
+  if (lane == 0 && emf) emf[k] = DIR == 0 ? -res[6] : res[5];
   if (spd) {
     rate = fmax(rate, __shfl_xor_sync(gmask, rate, 1, 4));
     rate = fmax(rate, __shfl_xor_sync(gmask, rate, 2, 4));
     if (lane == 0) spd[k] = rate;
   }
+  if (!nj) return;  // uniform over the block
   // no-jump proof over the 2H+1 transverse taps (mapped like every CT table
   // read), split across the group.  A tap whose mapped face is the one staged
   // in its tile slot reads the staged comparison; the others read memory.
@@ -2323,6 +2350,312 @@ void launch_face_lists(const Grid& g, const unsigned char* flag, int* xlist, int
                        int* counts, cudaStream_t s) {
   cudaMemsetAsync(counts, 0, 2 * sizeof(int), s);
   k_face_lists<<<cdiv(g.size(), 256), 256, 0, s>>>(g, flag, xlist, ylist, counts);
+}
+
+// ===========================================================================
+// Kernels of the per-kernel launch interface (reference
+// include/quasar/physics/mhd/kernels.hpp): the pieces that the fused step
+// above combines (flux difference, EMF curl, stage combine) as separate
+// launches, plus standalone forms of the reductions and fills.  Each uses the
+// arithmetic of the fused kernel it stands beside, so a step composed from
+// these launches reproduces the fused step.
+// ===========================================================================
+namespace {
+
+// Never written: the status word every stage kernel polls reads 0.
+__device__ Ctl g_abi_zero_ctl;
+
+// dudt += -(F_hi - F_lo)/h over the interior cells, all eight slots
+// (mhd_update.hip:21-105).
+__global__ void __launch_bounds__(256) k_abi_flux_difference(Grid g, FluxP f, int dir, FluxP d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const long long k = g.idx(i, j), kp = k + (dir == 0 ? 1 : g.pitch);
+  const double h = dir == 0 ? g.dx : g.dy;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const double dq = __dadd_rn(__ddiv_rn(f.f[q][kp], h), __ddiv_rn(-f.f[q][k], h));
+    d.f[q][k] = __dadd_rn(d.f[q][k], -dq);
+  }
+}
+
+// dudt.bx_face / dudt.by_face = curl of the corner E_z, overwritten
+// (mhd_ct.hip:893-931): bx on i <= nx, j < ny; by on i < nx, j <= ny.
+__global__ void __launch_bounds__(256) k_abi_curl_rate(Grid g, const double* __restrict__ ez,
+                                                       double* dbx, double* dby) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > g.nx || j > g.ny) return;
+  const long long k = g.idx(i, j);
+  if (j < g.ny) dbx[k] = __dadd_rn(__ddiv_rn(-ez[k + g.pitch], g.dy), __ddiv_rn(ez[k], g.dy));
+  if (i < g.nx) dby[k] = __dadd_rn(__ddiv_rn(ez[k + 1], g.dx), __ddiv_rn(-ez[k], g.dx));
+}
+
+// out = a un + b us + c dudt (mhd_update.hip:113-206): an operand whose weight
+// is zero is not read, (1, 0, 0) is an exact copy; cell components over the
+// interior, bx also on i = nx and by on j = ny.
+__global__ void __launch_bounds__(256) k_abi_rk_stage(Grid g, StateP out, StateP un, StateP us,
+                                                      FluxP d, double a, double b, double c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > g.nx || j > g.ny) return;
+  const long long k = g.idx(i, j);
+  const bool copy = a == 1.0 && b == 0.0 && c == 0.0;
+  const bool ua = a != 0.0, ub = b != 0.0, uc = c != 0.0;
+  auto comb = [&](int q) {
+    if (copy) return un.c[q][k];
+    if (ua && ub && uc)
+      return crsum3(__dmul_rn(a, un.c[q][k]), __dmul_rn(b, us.c[q][k]), __dmul_rn(c, d.f[q][k]));
+    if (ua && ub) return __dadd_rn(__dmul_rn(a, un.c[q][k]), __dmul_rn(b, us.c[q][k]));
+    if (ua && uc) return __dadd_rn(__dmul_rn(a, un.c[q][k]), __dmul_rn(c, d.f[q][k]));
+    if (ub && uc) return __dadd_rn(__dmul_rn(b, us.c[q][k]), __dmul_rn(c, d.f[q][k]));
+    if (ua) return __dmul_rn(a, un.c[q][k]);
+    if (ub) return __dmul_rn(b, us.c[q][k]);
+    if (uc) return __dmul_rn(c, d.f[q][k]);
+    return 0.0;
+  };
+  if (i < g.nx && j < g.ny) {
+    const int cc[6] = {0, 1, 2, 3, 4, 7};
+#pragma unroll
+    for (int t = 0; t < 6; ++t) out.c[cc[t]][k] = comb(cc[t]);
+  }
+  if (j < g.ny) out.c[5][k] = comb(5);
+  if (i < g.nx) out.c[6][k] = comb(6);
+}
+
+// Face -> cell collocation of one axis over the padded grid
+// (launch_mhd_collocate_face_to_cell, mhd_staggering.hpp:77-236).
+template <int W>
+__global__ void k_abi_collocate(Grid g, int axis, const double* __restrict__ face,
+                                double* __restrict__ cell) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - g.ng;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - g.ng;
+  if (i >= g.nx + g.ng || j >= g.ny + g.ng) return;
+  cell[g.idx(i, j)] = axis == 0
+                          ? face_to_cell<W>(face, (long long)g.idx(0, j), 1, i, -g.ng, g.nx + g.ng - 1)
+                          : face_to_cell<W>(face, (long long)g.idx(i, 0), g.pitch, j, -g.ng,
+                                            g.ny + g.ng - 1);
+}
+
+// One side's ghost layers, fluid (parts 1) or field (parts 2)
+// (mhd_boundary_hip.hip:66-218).
+__global__ void k_abi_fill_side(Grid g, StateP u, int side, int mode, int parts) {
+  const int axis = side / 2;
+  const int lines = (axis == 0 ? g.ny : g.nx) + 2 * g.ng;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ng * lines) return;
+  fill_ghost(g, u, axis, (side & 1) == 0, mode, t / lines + 1, t % lines - g.ng, parts);
+}
+
+__device__ __forceinline__ void atomic_min_lanes(unsigned long long* dst, unsigned long long v) {
+  const cg::coalesced_group grp = cg::coalesced_threads();
+  const unsigned long long m = cg::reduce(grp, v, cg::less<unsigned long long>());
+  if (grp.thread_rank() == 0) atomicMin(dst, m);
+}
+
+// Cell state with the high-order (coll 0) or two-face (coll 1) collocated
+// in-plane field, formed from the face arrays (mhd_staggering.hpp:321-338).
+template <int W>
+__device__ __forceinline__ St abi_cell(const Grid& g, const StateP& u, int i, int j, int coll) {
+  if (coll) return load_cell1(u, g, i, j);
+  const long long k = g.idx(i, j);
+  return St{u.c[0][k], u.c[1][k], u.c[2][k], u.c[3][k], u.c[4][k],
+            face_to_cell<W>(u.c[5], (long long)g.idx(0, j), 1, i, -g.ng, g.nx + g.ng - 1),
+            face_to_cell<W>(u.c[6], (long long)g.idx(i, 0), g.pitch, j, -g.ng, g.ny + g.ng - 1),
+            u.c[7][k]};
+}
+
+// Admissible convex fraction with density and internal-energy floors
+// (mhd_reduce.hip:143-209); *theta holds the bits of the running minimum.
+template <int W>
+__global__ void __launch_bounds__(256) k_abi_admissible(Grid g, StateP base, StateP cand,
+                                                        double rho_floor, double q_floor,
+                                                        int coll, unsigned long long* theta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const St a = abi_cell<W>(g, base, i, j, coll), b = abi_cell<W>(g, cand, i, j, coll);
+  double local = 1.0;
+  const double qa = convex_q(a, b, 0.0);
+  if (!(a.rho > rho_floor) || !(qa > q_floor) || !isfinite(a.rho) || !isfinite(qa)) {
+    local = 0.0;
+  } else if (!(isfinite(b.rho) && isfinite(b.mx) && isfinite(b.my) && isfinite(b.mz) &&
+               isfinite(b.E) && isfinite(b.bx) && isfinite(b.by) && isfinite(b.bz))) {
+    local = 0.0;
+  } else {
+    double hi = 1.0;
+    if (b.rho <= rho_floor) {
+      const double den = a.rho - b.rho;
+      hi = den > 0.0 ? (a.rho - rho_floor) / den : 0.0;
+      hi = fmin(fmax(hi, 0.0), 1.0);
+    }
+    if (convex_q(a, b, hi) > q_floor) {
+      local = hi;
+    } else {
+      double lo = 0.0;
+      for (int it = 0; it < 56; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (convex_q(a, b, mid) > q_floor) lo = mid;
+        else hi = mid;
+      }
+      local = lo;
+    }
+  }
+  atomic_min_lanes(theta, dbits(local));
+}
+
+// Relative solenoidality of the interior cells: acc[0] residual, acc[1]
+// scale maxima (bits).
+__global__ void __launch_bounds__(256) k_abi_divb_relative(Grid g, StateP u, int solver_owned,
+                                                           unsigned long long* acc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  unsigned long long rb, sb;
+  divb_cell(g, u, g.idx(i, j), solver_owned, rb, sb);
+  atomic_max_lanes(acc, rb);
+  atomic_max_lanes(acc + 1, sb);
+}
+
+// CFL rate 0.5 alpha / h of the face with high cell (i, j) normal to DIR, as
+// the face-flux kernels form it: the face-average Riemann problem and, for
+// MP5/MP7, every Gauss point before the first inadmissible one
+// (mhd_reduce.hip:254-416).
+template <int DIR, int ORDER>
+__device__ double abi_face_rate(const Grid& g, const IfaceP& in, int i, int j, double gamma) {
+  int si = i, sj = j;
+  if (DIR == 0 && i == g.nx && g.bc[0] == 0 && g.bc[1] == 0) si = 0;
+  if (DIR == 1 && j == g.ny && g.bc[2] == 0 && g.bc[3] == 0) sj = 0;
+  const long long ks = g.idx(si, sj);
+  const double h = DIR == 0 ? g.dx : g.dy;
+  double rate = face_rate<DIR, ORDER>(iface(in, ks, true), iface(in, ks, false), gamma, h);
+  if (ORDER != 5 && ORDER != 7) return rate;
+  constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
+  const long long ts = DIR == 0 ? g.pitch : 1;
+  for (int q = 0; q < Q; ++q) {
+    double w[N];
+#pragma unroll
+    for (int t = 0; t < N; ++t) w[t] = point_w<ORDER>(q, t);
+    double pl[8], pr[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      double sa[N], sb[N];
+#pragma unroll
+      for (int t = 0; t < N; ++t) {
+        sa[t] = in.L[c][ks + (t - H) * ts];
+        sb[t] = in.R[c][ks + (t - H) * ts];
+      }
+      pl[c] = wsum<N>(w, sa);
+      pr[c] = wsum<N>(w, sb);
+    }
+    const St l{pl[0], pl[1], pl[2], pl[3], pl[4], pl[5], pl[6], pl[7]};
+    const St r{pr[0], pr[1], pr[2], pr[3], pr[4], pr[5], pr[6], pr[7]};
+    if (!point_admissible(l, gamma) || !point_admissible(r, gamma)) break;
+    rate = fmax(rate, face_rate<DIR, ORDER>(l, r, gamma, h));
+  }
+  return rate;
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(256) k_abi_cfl_rate(Grid g, IfaceP ix, IfaceP iy, double gamma,
+                                                      unsigned long long* max_rate) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const double r = (abi_face_rate<0, ORDER>(g, ix, i, j, gamma) +
+                    abi_face_rate<0, ORDER>(g, ix, i + 1, j, gamma)) +
+                   (abi_face_rate<1, ORDER>(g, iy, i, j, gamma) +
+                    abi_face_rate<1, ORDER>(g, iy, i, j + 1, gamma));
+  const double local = isfinite(r) ? fmax(0.0, r) : kInf;
+  atomic_max_lanes(max_rate, dbits(local));
+}
+
+__global__ void k_abi_set_u64(unsigned long long* p, int n, unsigned long long v) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) p[t] = v;
+}
+
+std::mutex g_abi_mu;
+Ctl* g_abi_ctl_ptr[64] = {};
+
+}  // namespace
+
+cudaError_t abi_zero_ctl(Ctl** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_abi_mu);
+  if (!g_abi_ctl_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_abi_zero_ctl);
+    if (e != cudaSuccess) return e;
+    g_abi_ctl_ptr[dev] = static_cast<Ctl*>(p);
+  }
+  *out = g_abi_ctl_ptr[dev];
+  return cudaSuccess;
+}
+
+void launch_abi_flux_difference(const Grid& g, const FluxP& f, int dir, const FluxP& d,
+                                cudaStream_t s) {
+  k_abi_flux_difference<<<dim3(cdiv(g.nx, kBX), cdiv(g.ny, 8)), dim3(kBX, 8), 0, s>>>(g, f, dir, d);
+}
+
+void launch_abi_curl_rate(const Grid& g, const double* ez, double* dbx, double* dby,
+                          cudaStream_t s) {
+  k_abi_curl_rate<<<dim3(cdiv(g.nx + 1, kBX), cdiv(g.ny + 1, 8)), dim3(kBX, 8), 0, s>>>(g, ez, dbx,
+                                                                                       dby);
+}
+
+void launch_abi_rk_stage(const Grid& g, const StateP& out, const StateP& un, const StateP& us,
+                         const FluxP& d, double a, double b, double c, cudaStream_t s) {
+  k_abi_rk_stage<<<dim3(cdiv(g.nx + 1, kBX), cdiv(g.ny + 1, 8)), dim3(kBX, 8), 0, s>>>(
+      g, out, un, us, d, a, b, c);
+}
+
+void launch_abi_collocate(const Grid& g, int axis, const double* face, double* cell,
+                          cudaStream_t s) {
+  const dim3 grid(cdiv(g.nx + 2 * g.ng, kBX), cdiv(g.ny + 2 * g.ng, 8)), block(kBX, 8);
+  if (g.ng == 2) k_abi_collocate<4><<<grid, block, 0, s>>>(g, axis, face, cell);
+  else if (g.ng == 3) k_abi_collocate<6><<<grid, block, 0, s>>>(g, axis, face, cell);
+  else k_abi_collocate<8><<<grid, block, 0, s>>>(g, axis, face, cell);
+}
+
+void launch_abi_fill_side(const Grid& g, const StateP& u, int side, int mode, int parts,
+                          cudaStream_t s) {
+  const long long n = (long long)g.ng * ((side / 2 == 0 ? g.ny : g.nx) + 2 * g.ng);
+  k_abi_fill_side<<<cdiv(n, 256), 256, 0, s>>>(g, u, side, mode, parts);
+}
+
+void launch_abi_admissible(const Grid& g, const StateP& base, const StateP& cand,
+                           double rho_floor, double q_floor, int coll, unsigned long long* theta,
+                           cudaStream_t s) {
+  const dim3 grid(cdiv(g.nx, kBX), cdiv(g.ny, 8)), block(kBX, 8);
+  if (g.ng == 2) k_abi_admissible<4><<<grid, block, 0, s>>>(g, base, cand, rho_floor, q_floor, coll, theta);
+  else if (g.ng == 3) k_abi_admissible<6><<<grid, block, 0, s>>>(g, base, cand, rho_floor, q_floor, coll, theta);
+  else k_abi_admissible<8><<<grid, block, 0, s>>>(g, base, cand, rho_floor, q_floor, coll, theta);
+}
+
+void launch_abi_divb_relative(const Grid& g, const StateP& u, int solver_owned,
+                              unsigned long long* acc, cudaStream_t s) {
+  k_abi_divb_relative<<<dim3(cdiv(g.nx, kBX), cdiv(g.ny, 8)), dim3(kBX, 8), 0, s>>>(
+      g, u, solver_owned, acc);
+}
+
+void launch_abi_cfl_rate(const Grid& g, const IfaceP& ix, const IfaceP& iy, int order,
+                         double gamma, unsigned long long* max_rate, cudaStream_t s) {
+  const dim3 grid(cdiv(g.nx, kBX), cdiv(g.ny, 8)), block(kBX, 8);
+  switch (order) {
+    case 1: k_abi_cfl_rate<1><<<grid, block, 0, s>>>(g, ix, iy, gamma, max_rate); break;
+    case 2: k_abi_cfl_rate<2><<<grid, block, 0, s>>>(g, ix, iy, gamma, max_rate); break;
+    case 5: k_abi_cfl_rate<5><<<grid, block, 0, s>>>(g, ix, iy, gamma, max_rate); break;
+    default: k_abi_cfl_rate<7><<<grid, block, 0, s>>>(g, ix, iy, gamma, max_rate);
+  }
+}
+
+void launch_abi_set_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s) {
+  k_abi_set_u64<<<cdiv(n, 256), 256, 0, s>>>(p, n, v);
 }
 
 }  // namespace qb

@@ -111,6 +111,33 @@ void launch_divb_linf(const Grid& g, const StateP& u, unsigned long long* out, c
 void launch_cell_sums(const Grid& g, const StateP& u, double* partial, int blocks,
                       cudaStream_t s);
 
+// ---- per-kernel launch interface (launch_abi.cu) ---------------------------
+// Device address of a zero control block that no kernel writes (the calling
+// thread's current device; looked up once per device).
+cudaError_t abi_zero_ctl(Ctl** out);
+void launch_abi_flux_difference(const Grid& g, const FluxP& f, int dir, const FluxP& d,
+                                cudaStream_t s);
+void launch_abi_curl_rate(const Grid& g, const double* ez, double* dbx, double* dby,
+                          cudaStream_t s);
+void launch_abi_rk_stage(const Grid& g, const StateP& out, const StateP& un, const StateP& us,
+                         const FluxP& d, double a, double b, double c, cudaStream_t s);
+void launch_abi_collocate(const Grid& g, int axis, const double* face, double* cell,
+                          cudaStream_t s);
+// parts: 1 fluid components, 2 staggered field
+void launch_abi_fill_side(const Grid& g, const StateP& u, int side, int mode, int parts,
+                          cudaStream_t s);
+// *theta: bits of the running minimum (start it at the bits of 1.0)
+void launch_abi_admissible(const Grid& g, const StateP& base, const StateP& cand,
+                           double rho_floor, double q_floor, int coll, unsigned long long* theta,
+                           cudaStream_t s);
+// acc[0], acc[1]: bits of the residual and scale maxima (start them at 0)
+void launch_abi_divb_relative(const Grid& g, const StateP& u, int solver_owned,
+                              unsigned long long* acc, cudaStream_t s);
+// *max_rate: bits of the running maximum (start it at 0)
+void launch_abi_cfl_rate(const Grid& g, const IfaceP& ix, const IfaceP& iy, int order,
+                         double gamma, unsigned long long* max_rate, cudaStream_t s);
+void launch_abi_set_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s);
+
 // ---- batched step: many independent instances per launch -----------------
 // One record per instance and stage: the instance's stage arguments (a.u is
 // the stage input), its live register (update and admissibility base) and the

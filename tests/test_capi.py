@@ -36,6 +36,68 @@ def test_library_exports_every_declared_symbol():
     ext = declared_symbols("quasar_mhd_ext.h")
     assert set(ext) == set(_native.EXT_EXPORTS)
     assert all(hasattr(lib, s) for s in ext)
+    launch = declared_symbols("quasar_mhd_launch.h")
+    assert set(launch) == set(_native.LAUNCH_EXPORTS)
+    assert all(hasattr(lib, s) for s in launch)
+
+
+def test_launch_interface_names_every_reference_seam_entry():
+    # kernels.hpp entry points of the Cartesian, zero-background hot path
+    want = ("reconstruct", "hlld_flux", "flux_difference", "ct_emf_prepare", "ct_emf_finish",
+            "emf_curl_rate", "rk_stage", "admissible_fraction", "cfl_max_rate", "ct_divb_linf",
+            "ct_divb_relative_linf", "fill_ghosts_fluid", "fill_ghosts_field",
+            "collocate_face_to_cell", "conserved_cell_sums")
+    assert set("qmhd_launch_" + w for w in want) == set(declared_symbols("quasar_mhd_launch.h"))
+
+
+def test_launch_interface_rejects_bad_arguments_before_any_launch():
+    """Host-side validation (null device pointers throughout, so nothing could
+    be launched even if a check were missing)."""
+    import pytest
+    from quasar_b200 import launch as L
+    g = L.Grid(16, 16, 4, 1 / 16, 1 / 16)
+    u, iface = L.Field(), L.Iface()
+    per = L.flags((0, 0, 0, 0))
+    with pytest.raises(ValueError, match="dir"):
+        L.reconstruct(g, u, None, None, 2, iface, 7, per, 5 / 3, stream=0)
+    with pytest.raises(ValueError, match="nghost"):
+        L.reconstruct(g, u, None, None, 0, iface, 5, per, 5 / 3, stream=0)
+    with pytest.raises(ValueError, match="periodic"):
+        L.reconstruct(g, u, None, None, 0, iface, 7, L.flags((0, 1, 0, 0)), 5 / 3, stream=0)
+    with pytest.raises(ValueError, match="boundary flag"):
+        L.hlld_flux(g, iface, 0, u, L.flags((3, 3, 0, 0)), 5 / 3, 7, stream=0)
+    with pytest.raises(ValueError, match="gamma"):
+        L.hlld_flux(g, iface, 0, u, per, 1.0, 7, stream=0)
+    with pytest.raises(ValueError, match="null"):
+        L.hlld_flux(g, iface, 0, u, per, 5 / 3, 7, stream=0)
+    with pytest.raises(ValueError, match="null"):
+        L.flux_difference(g, u, 0, u, stream=0)
+    import ctypes
+    from quasar_b200 import _native
+    lib = _native.lib()
+    with pytest.raises(ValueError, match="side"):
+        _native.check(lib.qmhd_launch_fill_ghosts_fluid(ctypes.byref(g), ctypes.byref(u), 5, 0,
+                                                        None))
+    with pytest.raises(ValueError, match="mode"):
+        _native.check(lib.qmhd_launch_fill_ghosts_field(ctypes.byref(g), ctypes.byref(u), 1, 3,
+                                                        None))
+    with pytest.raises(ValueError, match="nghost must be"):
+        L.collocate_face_to_cell(L.Grid(16, 16, 6, 1 / 16, 1 / 16), 0, None, None, stream=0)
+    with pytest.raises(ValueError, match="scratch"):
+        L.ct_divb_linf(g, u, None, stream=0)
+    with pytest.raises(ValueError, match="cylindrical"):
+        _native.check(lib.qmhd_launch_flux_difference(ctypes.byref(g), ctypes.byref(u), 0,
+                                                      ctypes.byref(u), None, 1))
+    with pytest.raises(ValueError, match="rate-only"):
+        _native.check(lib.qmhd_launch_reconstruct(ctypes.byref(g), ctypes.byref(u), None, None, 0,
+                                                  ctypes.byref(iface), 7, per, 5 / 3, None, 1))
+    with pytest.raises(ValueError, match="ownership"):
+        _native.check(lib.qmhd_launch_hlld_flux(ctypes.byref(g), ctypes.byref(iface), 0,
+                                                ctypes.byref(u), per, 5 / 3, None, 0, 7,
+                                                L.flags((1, 0, 1, 1))))
+    with pytest.raises(ValueError, match="hll_only"):
+        _native.check(lib.qmhd_launch_hlld_flux(ctypes.byref(g), ctypes.byref(iface), 0,
+                                                ctypes.byref(u), per, 5 / 3, None, 1, 7, None))
 
 
 def test_python_config_validation_matches_reference_errors():
