@@ -1079,26 +1079,29 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
 // a face.  Each lane recovers its point state and solves its Riemann problem;
 // the group votes on admissibility, gathers the point fluxes in node order for
 // the Gauss sum, and splits the stores.  Same arithmetic as k_face_flux (node
-// order of every sum kept).  The interface states of a 16 x 4 face tile and
+// order of every sum kept).  The interface states of an 8 x 4 face tile and
 // its transverse halo are staged in shared memory, so each stencil row is
 // read from L2 once per tile instead of once per face row (2.8x fewer for x
-// faces, 5x for y faces at MP7).  256 threads: 64 faces x 4 Gauss lanes.
+// faces, 4x for y faces at MP7).  128 threads: 32 faces x 4 Gauss lanes, four
+// blocks per SM (smaller blocks than 16 x 4 measured 3-5% faster: a block
+// waiting at the staging barrier holds fewer warps).
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr int kFqTX = 16, kFqTY = 4;
+constexpr int kFqTX = 8, kFqTY = 4;
 
-template <int DIR, int ORDER>
+// TX: faces per tile row; the block has 4 * TX * kFqTY threads.
+template <int DIR, int ORDER, int TX = kFqTX>
 __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, const FluxP& out,
                                                double* emf, int* nj, double* spd, double gamma,
                                                const Ctl* ctl, int bx, int by) {
   constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
   constexpr int TR = DIR == 0 ? kFqTY + 2 * H : kFqTY;   // tile rows (j)
-  constexpr int TC = DIR == 0 ? kFqTX : kFqTX + 2 * H;   // tile columns (i)
+  constexpr int TC = DIR == 0 ? TX : TX + 2 * H;         // tile columns (i)
   __shared__ double tile[16][TR][TC];
   __shared__ unsigned char same[TR][TC];  // staged and L == R in every component
   if (ctl->status) return;  // uniform over the block
-  const int i0 = bx * kFqTX, j0 = by * kFqTY;
+  const int i0 = bx * TX, j0 = by * kFqTY;
   const bool perx = g.bc[0] == 0 && g.bc[1] == 0, pery = g.bc[2] == 0 && g.bc[3] == 0;
   for (int e = threadIdx.x; e < TR * TC; e += blockDim.x) {
     const int row = e / TC, col = e - row * TC;
@@ -1131,7 +1134,7 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
   constexpr bool kLF = false;
   const int lane = threadIdx.x & 3, grp = threadIdx.x >> 2;
   const unsigned gmask = 0xFu << (threadIdx.x & 28);
-  const int fx = grp % kFqTX, fy = grp / kFqTX;
+  const int fx = grp % TX, fy = grp / TX;
   const int i = i0 + fx, j = j0 + fy;
   if (i > g.nx || j > g.ny) return;  // whole four-lane groups leave together
   const long long k = g.idx(i, j);
@@ -1241,10 +1244,11 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(256, 2) k_face_flux_qs(Grid g, IfaceP in, FluxP out, double* emf,
-                                                         int* nj, double* spd, double gamma,
-                                                         const Ctl* ctl) {
-  b_face_flux_qs<DIR, ORDER>(g, in, out, emf, nj, spd, gamma, ctl, blockIdx.x, blockIdx.y);
+__global__ void __launch_bounds__(4 * kFqTX * kFqTY, 512 / (4 * kFqTX * kFqTY))
+    k_face_flux_qs(Grid g, IfaceP in, FluxP out, double* emf, int* nj, double* spd, double gamma,
+                   const Ctl* ctl) {
+  b_face_flux_qs<DIR, ORDER, kFqTX>(g, in, out, emf, nj, spd, gamma, ctl, blockIdx.x,
+                                          blockIdx.y);
 }
 
 }  // namespace
@@ -1555,7 +1559,12 @@ __device__ __forceinline__ void b_corner_emf_s(const Grid& g, const double* cell
   constexpr int LO = ORDER >= 7 ? -4 : ORDER >= 5 ? -3 : -1;
   constexpr int NT = ORDER >= 7 ? 8 : ORDER >= 5 ? 6 : 2;
   constexpr int TW = 32 + NT - 1, TH = 4 + NT - 1;
+  // the block's mapped stencils: cell E_z (TH x TW), the x-face E_z and proofs
+  // of its 32 corner columns over TH rows, the y-face ones of its 4 corner
+  // rows over TW columns
   __shared__ double tile[TH][TW];
+  __shared__ double sxe[TH][32], sye[4][TW];
+  __shared__ int sxn[TH][32], syn[4][TW];
   if (ctl->status) return;  // uniform over the block
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
   const int i0 = bx * 32, j0 = by * 4;
@@ -1564,6 +1573,22 @@ __device__ __forceinline__ void b_corner_emf_s(const Grid& g, const double* cell
     const int mi = face_index(i0 + LO + a, g.nx, g.bc[0], g.bc[1]);
     const int mj = face_index(j0 + LO + b, g.ny, g.bc[2], g.bc[3]);
     tile[b][a] = __ldg(cell_ez + g.idx(mi, mj));
+  }
+  for (int t = tid; t < TH * 32; t += 128) {
+    const int a = t % 32, b = t / 32;
+    const int fi = face_index(i0 + a, g.nx, g.bc[0], g.bc[1]);
+    const int mj = face_index(j0 + LO + b, g.ny, g.bc[2], g.bc[3]);
+    const long long kx = g.idx(fi, mj);
+    sxe[b][a] = __ldg(xemf + kx);
+    sxn[b][a] = __ldg(xnj + kx);
+  }
+  for (int t = tid; t < 4 * TW; t += 128) {
+    const int a = t % TW, b = t / TW;
+    const int mi = face_index(i0 + LO + a, g.nx, g.bc[0], g.bc[1]);
+    const int fj = face_index(j0 + b, g.ny, g.bc[2], g.bc[3]);
+    const long long ky = g.idx(mi, fj);
+    sye[b][a] = __ldg(yemf + ky);
+    syn[b][a] = __ldg(ynj + ky);
   }
   __syncthreads();
   const int i = i0 + tx, j = j0 + ty;
@@ -1575,24 +1600,18 @@ __device__ __forceinline__ void b_corner_emf_s(const Grid& g, const double* cell
     ez[k] = 0.0;
     return;
   }
-  const int fi = face_index(i, g.nx, g.bc[0], g.bc[1]);
-  const int fj = face_index(j, g.ny, g.bc[2], g.bc[3]);
   double e[NT], line[NT];
   bool nj_y = true, nj_x = true;
 #pragma unroll
   for (int q = 0; q < NT; ++q) {
-    const int mj = face_index(j + LO + q, g.ny, g.bc[2], g.bc[3]);
-    const long long kx = g.idx(fi, mj);
-    e[q] = __ldg(xemf + kx);
-    nj_x = nj_x && __ldg(xnj + kx) != 0;
+    e[q] = sxe[ty + q][tx];
+    nj_x = nj_x && sxn[ty + q][tx] != 0;
   }
   const double ex = edge_interp<NT>(e);
 #pragma unroll
   for (int q = 0; q < NT; ++q) {
-    const int mi = face_index(i + LO + q, g.nx, g.bc[0], g.bc[1]);
-    const long long ky = g.idx(mi, fj);
-    e[q] = __ldg(yemf + ky);
-    nj_y = nj_y && __ldg(ynj + ky) != 0;
+    e[q] = sye[ty][tx + q];
+    nj_y = nj_y && syn[ty][tx + q] != 0;
   }
   const double ey = edge_interp<NT>(e);
   bool const_x = true, const_y = true;
@@ -1884,13 +1903,13 @@ __global__ void kb_face_lists(const BatchRec* __restrict__ r, const BatchLearnRe
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(256, 2) kb_face_flux_q(const BatchRec* __restrict__ r,
-                                                         BatchPlan p, int speeds) {
+__global__ void __launch_bounds__(4 * kFqTX * kFqTY, 512 / (4 * kFqTX * kFqTY))
+    kb_face_flux_q(const BatchRec* __restrict__ r, BatchPlan p, int speeds) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
     int local, bx, by;
     const BatchRec& q = r[batch_locate(p, t, &local)];
     batch_block(kBpFlux, q.a.g, local, &bx, &by);
-    b_face_flux_qs<DIR, ORDER>(q.a.g, DIR == 0 ? q.a.ix : q.a.iy, DIR == 0 ? q.a.fx : q.a.fy,
+    b_face_flux_qs<DIR, ORDER, kFqTX>(q.a.g, DIR == 0 ? q.a.ix : q.a.iy, DIR == 0 ? q.a.fx : q.a.fy,
                                DIR == 0 ? q.a.xemf : q.a.yemf, DIR == 0 ? q.a.xnj : q.a.ynj,
                                speeds ? (DIR == 0 ? q.a.xspd : q.a.yspd) : nullptr, q.a.gamma,
                                q.a.ctl, bx, by);
@@ -2046,7 +2065,7 @@ static void flux_launch(const StageArgs& a, bool speeds, cudaStream_t s) {
   const Grid& g = a.g;
   if (ORDER == 5 || ORDER == 7) {
     const dim3 grid(cdiv(g.nx + 1, kFqTX), cdiv(g.ny + 1, kFqTY));
-    k_face_flux_qs<DIR, ORDER == 5 ? 5 : 7><<<grid, 256, 0, s>>>(
+    k_face_flux_qs<DIR, ORDER == 5 ? 5 : 7><<<grid, 4 * kFqTX * kFqTY, 0, s>>>(
         g, DIR == 0 ? a.ix : a.iy, DIR == 0 ? a.fx : a.fy, DIR == 0 ? a.xemf : a.yemf,
         DIR == 0 ? a.xnj : a.ynj, speeds ? (DIR == 0 ? a.xspd : a.yspd) : nullptr, a.gamma, a.ctl);
     return;
@@ -2164,6 +2183,7 @@ void batch_cell_configure() {
 int batch_phase_threads(int phase) {
   switch (phase) {
     case kBpRecon0: case kBpRecon1: case kBpCorner: return 128;
+    case kBpFlux: return 4 * kFqTX * kFqTY;
     default: return 256;
   }
 }
@@ -2181,7 +2201,10 @@ int batch_phase_max_ctas_per_sm(int phase, int order) {
       ensure_smem((const void*)kb_reconstruct<1, 5>, kReconSmem);
       return o7 ? max_ctas(kb_reconstruct<1, 7>, 128, kReconSmem)
                 : max_ctas(kb_reconstruct<1, 5>, 128, kReconSmem);
-    case kBpFlux: return o7 ? max_ctas(kb_face_flux_q<0, 7>, 256, 0) : max_ctas(kb_face_flux_q<0, 5>, 256, 0);
+    case kBpFlux: {
+      constexpr int t = 4 * kFqTX * kFqTY;
+      return o7 ? max_ctas(kb_face_flux_q<0, 7>, t, 0) : max_ctas(kb_face_flux_q<0, 5>, t, 0);
+    }
     case kBpCell:
       if (o7) {
         batch_cell_configure<7>();
@@ -2222,11 +2245,11 @@ void launch_batch_face_flux(const BatchRec* r, const BatchPlan& p, int dir, int 
                             bool speeds, cudaStream_t s) {
   const int sp = speeds ? 1 : 0;
   if (order == 7) {
-    if (dir == 0) kb_face_flux_q<0, 7><<<pgrid(p), 256, 0, s>>>(r, p, sp);
-    else kb_face_flux_q<1, 7><<<pgrid(p), 256, 0, s>>>(r, p, sp);
+    if (dir == 0) kb_face_flux_q<0, 7><<<pgrid(p), 4 * kFqTX * kFqTY, 0, s>>>(r, p, sp);
+    else kb_face_flux_q<1, 7><<<pgrid(p), 4 * kFqTX * kFqTY, 0, s>>>(r, p, sp);
   } else {
-    if (dir == 0) kb_face_flux_q<0, 5><<<pgrid(p), 256, 0, s>>>(r, p, sp);
-    else kb_face_flux_q<1, 5><<<pgrid(p), 256, 0, s>>>(r, p, sp);
+    if (dir == 0) kb_face_flux_q<0, 5><<<pgrid(p), 4 * kFqTX * kFqTY, 0, s>>>(r, p, sp);
+    else kb_face_flux_q<1, 5><<<pgrid(p), 4 * kFqTX * kFqTY, 0, s>>>(r, p, sp);
   }
 }
 
