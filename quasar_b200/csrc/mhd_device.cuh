@@ -577,10 +577,13 @@ __constant__ double c_point7[4][7] = {
 // centre one return it unchanged (finite_volume_quadrature.hpp:55-68).
 template <int N>
 __device__ __forceinline__ double wsum(const double* w, const double* s) {
+  // the centre is not compared with itself: a NaN centre equals no other
+  // sample either, so the decision is the same
   const double ref = s[N / 2];
   bool constant = true;
 #pragma unroll
-  for (int q = 0; q < N; ++q) constant = constant && (s[q] == ref);
+  for (int q = 0; q < N; ++q)
+    if (q != N / 2) constant = constant && (s[q] == ref);
   if (constant) return ref;
   double sum = w[0] * s[0];
 #pragma unroll
