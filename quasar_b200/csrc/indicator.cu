@@ -631,10 +631,17 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
     for (int c0 = 0; c0 < kHidden; c0 += 16) {
       float z[16];
       tc::tmem_ld16(tc::tmem_addr(tb, warp * 32, c0), z);
+      // eight consecutive columns of a row are one 16-byte core-matrix row
 #pragma unroll
-      for (int c = 0; c < 16; ++c)
-        *reinterpret_cast<uint16_t*>(a1s + tc::kmajor_offset(row, c0 + c, kHidden)) =
-            to_bf16(gelu(z[c] + p.b1[c0 + c]));
+      for (int h = 0; h < 16; h += 8) {
+        uint32_t w[4];
+#pragma unroll
+        for (int c = 0; c < 8; c += 2)
+          w[c / 2] = uint32_t(to_bf16(gelu(z[h + c] + p.b1[c0 + h + c]))) |
+                     (uint32_t(to_bf16(gelu(z[h + c + 1] + p.b1[c0 + h + c + 1]))) << 16);
+        *reinterpret_cast<uint4*>(a1s + tc::kmajor_offset(row, c0 + h, kHidden)) =
+            make_uint4(w[0], w[1], w[2], w[3]);
+      }
     }
     tc::fence_async_smem();
     tc::fence_before_sync();

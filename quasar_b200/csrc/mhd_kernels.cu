@@ -659,47 +659,40 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
 // Component-wise unlimited MP interpolation of the same conserved deltas:
 // the characteristic path with L = R = I and no limiter, which equals the
 // characteristic result wherever the limiter accepts every wave (R L = I).
+// The components are independent, so each is loaded, interpolated and
+// finished before the next (few live registers); the sums are those of the
+// whole-state form.
 template <int DIR, int H>
 __device__ void mp_pair_lin(const StateP& u, long long k0, long long step, St& ul, St& ur) {
   constexpr int S = 2 * H + 2, W = 2 * H + 1;
-  const St cl = load_cell(u, k0 - step), cr = load_cell(u, k0);
-  St ref;
-  ref.rho = 0.5 * cl.rho + 0.5 * cr.rho;
-  ref.mx = 0.5 * cl.mx + 0.5 * cr.mx;
-  ref.my = 0.5 * cl.my + 0.5 * cr.my;
-  ref.mz = 0.5 * cl.mz + 0.5 * cr.mz;
-  ref.E = 0.5 * cl.E + 0.5 * cr.E;
-  ref.bx = 0.5 * cl.bx + 0.5 * cr.bx;
-  ref.by = 0.5 * cl.by + 0.5 * cr.by;
-  ref.bz = 0.5 * cl.bz + 0.5 * cr.bz;
-  const St c = rot<DIR>(ref);
-  double u7[S][7];
+  double dl[8], dr[8], cv[8];
+  // canonical frame: rho, m_n, m_t1, m_t2, E, b_n, b_t1, b_t2
 #pragma unroll
-  for (int s = 0; s < S; ++s) {
-    const St d = rot<DIR>(load_cell(u, k0 + (long long)(s - 1 - H) * step));
-    u7[s][0] = d.rho - c.rho;
-    u7[s][1] = d.mx - c.mx;
-    u7[s][2] = d.my - c.my;
-    u7[s][3] = d.mz - c.mz;
-    u7[s][4] = d.E - c.E;
-    u7[s][5] = d.by - c.by;
-    u7[s][6] = d.bz - c.bz;
+  for (int v = 0; v < 8; ++v) {
+    const double* a = v == 0 ? u.c[0]
+                      : v == 1 ? (DIR == 0 ? u.c[1] : u.c[2])
+                      : v == 2 ? (DIR == 0 ? u.c[2] : u.c[1])
+                      : v == 3 ? u.c[3]
+                      : v == 4 ? u.c[4]
+                      : v == 5 ? (DIR == 0 ? u.bxc : u.byc)
+                      : v == 6 ? (DIR == 0 ? u.byc : u.bxc)
+                               : u.c[7];
+    const double c = 0.5 * __ldg(a + k0 - step) + 0.5 * __ldg(a + k0);
+    cv[v] = c;
+    if (v == 5) continue;  // the normal field is not reconstructed
+    double w[S];
+#pragma unroll
+    for (int t = 0; t < S; ++t) w[t] = __ldg(a + k0 + (long long)(t - 1 - H) * step) - c;
+    dl[v] = mp_interp_plain<W>(w);
+    double wr[W];
+#pragma unroll
+    for (int t = 0; t < W; ++t) wr[t] = w[W - t];
+    dr[v] = mp_interp_plain<W>(wr);
   }
-  double dl[7], dr[7];
-#pragma unroll
-  for (int v = 0; v < 7; ++v) {
-    double win[W];
-#pragma unroll
-    for (int s = 0; s < W; ++s) win[s] = u7[s][v];
-    dl[v] = mp_interp_plain<W>(win);
-#pragma unroll
-    for (int s = 0; s < W; ++s) win[s] = u7[W - s][v];
-    dr[v] = mp_interp_plain<W>(win);
-  }
-  const St sl{c.rho + dl[0], c.mx + dl[1], c.my + dl[2], c.mz + dl[3],
-              c.E + dl[4],   c.bx,         c.by + dl[5], c.bz + dl[6]};
-  const St sr{c.rho + dr[0], c.mx + dr[1], c.my + dr[2], c.mz + dr[3],
-              c.E + dr[4],   c.bx,         c.by + dr[5], c.bz + dr[6]};
+  const St sl{cv[0] + dl[0], cv[1] + dl[1], cv[2] + dl[2], cv[3] + dl[3],
+              cv[4] + dl[4], cv[5],         cv[6] + dl[6], cv[7] + dl[7]};
+  const St sr{cv[0] + dr[0], cv[1] + dr[1], cv[2] + dr[2], cv[3] + dr[3],
+              cv[4] + dr[4], cv[5],         cv[6] + dr[6], cv[7] + dr[7]};
   ul = rot<DIR>(sl);
   ur = rot<DIR>(sr);
 }
@@ -761,14 +754,27 @@ __device__ __forceinline__ float limiter_departure(const St& a, const St& b) {
   return isfinite(d) ? float(d) : INFINITY;
 }
 
+// Learned-mode face list of one direction: the per-cell flags it was built
+// from (a face is listed when either of its cells is flagged), the list and
+// its device-resident count.
+struct FaceList {
+  const unsigned char* flag;
+  int* list;
+  int* count;
+};
+
 // One face's interface states.  MODE 0: the characteristic MP path; 1: the
 // same, also recording per cell the largest departure of a limited state
 // from the unlimited component-wise one (label[cell] = max, as float bits;
 // the left state's stencil is centred on the left cell);
-// 2: the unlimited component-wise path.  Orders 1 and 2 ignore MODE.
+// 2: the unlimited component-wise path; a face whose unlimited states are
+// not admissible is appended to `defer` for the characteristic pass that
+// follows (the plain step's path for it, fallbacks included) unless it is
+// listed already.  Orders 1 and 2 ignore MODE.
 template <int DIR, int ORDER, int MODE>
 __device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const IfaceP& out,
-                                           double gamma, int i, int j, int* label) {
+                                           double gamma, int i, int j, int* label,
+                                           FaceList defer = FaceList{}) {
   const long long k0 = g.idx(i, j);
   const long long step = DIR == 0 ? 1 : g.pitch;
   St ul, ur;
@@ -781,6 +787,11 @@ __device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const
     constexpr int H = ORDER == 5 ? 2 : 3;
     if constexpr (MODE == 2) {
       mp_pair_lin<DIR, H>(u, k0, step, ul, ur);
+      if (!recon_admissible(ul, gamma) || !recon_admissible(ur, gamma)) {
+        if (!defer.flag[k0 - step] && !defer.flag[k0])
+          defer.list[atomicAdd(defer.count, 1)] = int(k0);
+        return;
+      }
     } else {
       mp_pair_loop<DIR, H>(u, k0, step, gamma, ul, ur);
       if (MODE == 1) {
@@ -791,8 +802,10 @@ __device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const
         atomicMax(label + k0, __float_as_int(limiter_departure(ur, lr)));
       }
     }
-    if (!recon_admissible(ul, gamma) || !recon_admissible(ur, gamma))
-      muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
+    if constexpr (MODE != 2) {
+      if (!recon_admissible(ul, gamma) || !recon_admissible(ur, gamma))
+        muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
+    }
   }
   const double bn = (DIR == 0 ? u.c[5] : u.c[6])[k0];
   set_normal_b<DIR>(ul, bn);
@@ -823,13 +836,14 @@ __device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const
 template <int DIR, int ORDER, int MODE = 0>
 __device__ __forceinline__ void b_reconstruct(const Grid& g, const StateP& u, const IfaceP& out,
                                               double gamma, const Ctl* ctl, int bx, int by,
-                                              int* label = nullptr) {
+                                              int* label = nullptr,
+                                              FaceList defer = FaceList{}) {
   // dir 0: faces i in [0,nx] over all padded rows; dir 1: transposed.
   const int i = bx * blockDim.x + threadIdx.x - (DIR == 1 ? g.ng : 0);
   const int j = by * blockDim.y + threadIdx.y - (DIR == 0 ? g.ng : 0);
   if (DIR == 0 ? (i > g.nx || j >= g.ny + g.ng) : (i >= g.nx + g.ng || j > g.ny)) return;
   if (ctl->status & ~kStatusDone) return;
-  recon_face<DIR, ORDER, MODE>(g, u, out, gamma, i, j, label);
+  recon_face<DIR, ORDER, MODE>(g, u, out, gamma, i, j, label, defer);
 }
 
 template <int DIR, int ORDER>
@@ -846,11 +860,13 @@ __global__ void __launch_bounds__(128) k_reconstruct_label(Grid g, StateP u, Ifa
   b_reconstruct<DIR, ORDER, 1>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y, label);
 }
 
-// Learned mode, pass 1: every face by the unlimited component-wise path.
+// Learned mode, pass 1: every face by the unlimited component-wise path
+// (inadmissible ones deferred to pass 2).
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128) k_reconstruct_lin(Grid g, StateP u, IfaceP out,
-                                                         double gamma, const Ctl* ctl) {
-  b_reconstruct<DIR, ORDER, 2>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y);
+__global__ void __launch_bounds__(128, 5) k_reconstruct_lin(Grid g, StateP u, IfaceP out,
+                                                         double gamma, const Ctl* ctl,
+                                                         FaceList defer) {
+  b_reconstruct<DIR, ORDER, 2>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y, nullptr, defer);
 }
 
 // Learned mode, pass 2: the listed faces (padded linear index of the face's
@@ -1830,13 +1846,19 @@ __global__ void k_cell_sums(Grid g, StateP u, double* partial) {
 namespace {
 
 template <int DIR, int ORDER, int MODE = 0>
-__global__ void __launch_bounds__(128) kb_reconstruct(const BatchRec* __restrict__ r, BatchPlan p) {
+__global__ void __launch_bounds__(128) kb_reconstruct(const BatchRec* __restrict__ r, BatchPlan p,
+                                                      const BatchLearnRec* __restrict__ l = nullptr) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
     int local, bx, by;
-    const BatchRec& q = r[batch_locate(p, t, &local)];
+    const int inst = batch_locate(p, t, &local);
+    const BatchRec& q = r[inst];
     batch_block(DIR == 0 ? kBpRecon0 : kBpRecon1, q.a.g, local, &bx, &by);
+    FaceList defer{};
+    if (MODE == 2)
+      defer = FaceList{l[inst].flag, DIR == 0 ? l[inst].xlist : l[inst].ylist,
+                       l[inst].counts + DIR};
     b_reconstruct<DIR, ORDER, MODE>(q.a.g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma,
-                                    q.a.ctl, bx, by);
+                                    q.a.ctl, bx, by, nullptr, defer);
   }
 }
 
@@ -2304,21 +2326,21 @@ void launch_batch_reconstruct_learned(const BatchRec* r, const BatchLearnRec* l,
   const dim3 block(32, 4);
   if (order == 7) {
     if (dir == 0) {
-      kb_reconstruct<0, 7, 2><<<pgrid(p), block, 0, s>>>(r, p);
+      kb_reconstruct<0, 7, 2><<<pgrid(p), block, 0, s>>>(r, p, l);
       ensure_smem((const void*)kb_reconstruct_list<0, 7>, kReconSmem);
       kb_reconstruct_list<0, 7><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
     } else {
-      kb_reconstruct<1, 7, 2><<<pgrid(p), block, 0, s>>>(r, p);
+      kb_reconstruct<1, 7, 2><<<pgrid(p), block, 0, s>>>(r, p, l);
       ensure_smem((const void*)kb_reconstruct_list<1, 7>, kReconSmem);
       kb_reconstruct_list<1, 7><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
     }
   } else {
     if (dir == 0) {
-      kb_reconstruct<0, 5, 2><<<pgrid(p), block, 0, s>>>(r, p);
+      kb_reconstruct<0, 5, 2><<<pgrid(p), block, 0, s>>>(r, p, l);
       ensure_smem((const void*)kb_reconstruct_list<0, 5>, kReconSmem);
       kb_reconstruct_list<0, 5><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
     } else {
-      kb_reconstruct<1, 5, 2><<<pgrid(p), block, 0, s>>>(r, p);
+      kb_reconstruct<1, 5, 2><<<pgrid(p), block, 0, s>>>(r, p, l);
       ensure_smem((const void*)kb_reconstruct_list<1, 5>, kReconSmem);
       kb_reconstruct_list<1, 5><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
     }
@@ -2351,19 +2373,19 @@ void launch_reconstruct_label(const StageArgs& a, int dir, int* label, cudaStrea
 #undef QB_LBL
 }
 
-void launch_reconstruct_learned(const StageArgs& a, int dir, const int* list, const int* count,
-                                int list_grid, cudaStream_t s) {
+void launch_reconstruct_learned(const StageArgs& a, int dir, const unsigned char* flag, int* list,
+                                int* count, int list_grid, cudaStream_t s) {
   const dim3 block(kBX, 4);
   const IfaceP out = dir == 0 ? a.ix : a.iy;
-#define QB_LRN(D, O)                                                                          \
-  if (dir == D && a.order == O) {                                                            \
-    k_reconstruct_lin<D, O><<<recon_grid<D, O>(a.g), block, 0, s>>>(a.g, a.u, out, a.gamma,  \
-                                                                    a.ctl);                  \
-    ensure_smem((const void*)k_reconstruct_list<D, O>, kReconSmem);                           \
-    k_reconstruct_list<D, O><<<list_grid, 128, kReconSmem, s>>>(a.g, a.u, out, a.gamma, a.ctl, \
-                                                                list,                         \
-                                                       count);                               \
-    return;                                                                                  \
+  const FaceList defer{flag, list, count};
+#define QB_LRN(D, O)                                                                            \
+  if (dir == D && a.order == O) {                                                              \
+    k_reconstruct_lin<D, O><<<recon_grid<D, O>(a.g), block, 0, s>>>(a.g, a.u, out, a.gamma,    \
+                                                                    a.ctl, defer);             \
+    ensure_smem((const void*)k_reconstruct_list<D, O>, kReconSmem);                             \
+    k_reconstruct_list<D, O><<<list_grid, 128, kReconSmem, s>>>(a.g, a.u, out, a.gamma, a.ctl,   \
+                                                                list, count);                  \
+    return;                                                                                    \
   }
   QB_LRN(0, 5) QB_LRN(1, 5) QB_LRN(0, 7) QB_LRN(1, 7)
 #undef QB_LRN

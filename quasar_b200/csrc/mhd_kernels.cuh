@@ -256,9 +256,11 @@ void launch_batch_ctl(const BatchRec* r, int n, int what, double t, double t_end
 // state's scale.  The array must start at zero.
 void launch_reconstruct_label(const StageArgs& a, int dir, int* label, cudaStream_t s);
 // Unlimited component-wise reconstruction of every face, then the full
-// characteristic path for the listed faces (count on the device).
-void launch_reconstruct_learned(const StageArgs& a, int dir, const int* list, const int* count,
-                                int list_grid, cudaStream_t s);
+// characteristic path for the listed faces (count on the device).  Faces
+// whose unlimited states are not admissible are appended to the list (flag:
+// the per-cell flags the list was built from).
+void launch_reconstruct_learned(const StageArgs& a, int dir, const unsigned char* flag, int* list,
+                                int* count, int list_grid, cudaStream_t s);
 // Faces adjacent to a flagged cell (flag per padded cell) -> x / y lists;
 // counts[0..1] are reset first.
 void launch_face_lists(const Grid& g, const unsigned char* flag, int* xlist, int* ylist,
