@@ -354,9 +354,12 @@ __device__ __forceinline__ void b_colloc_check(const Grid& g, const StateP& cand
   }
 }
 
+// Three blocks per SM: the bisection and ulp paths that are rarely taken spill
+// at 80 registers, and the common path runs 22% faster than at 122 registers.
 template <int W>
-__global__ void k_colloc_check(Grid g, StateP cand, StateP base, int has_base, int theta_mask,
-                               int live_checks, int solver_owned, double gamma, Ctl* ctl) {
+__global__ void __launch_bounds__(256, 3)
+    k_colloc_check(Grid g, StateP cand, StateP base, int has_base, int theta_mask,
+                   int live_checks, int solver_owned, double gamma, Ctl* ctl) {
   b_colloc_check<W>(g, cand, base, has_base, theta_mask, live_checks, solver_owned, gamma, ctl, blockIdx.x,
                     blockIdx.y);
 }
@@ -1098,13 +1101,16 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
 // order of every sum kept).  The interface states of an 8 x 4 face tile and
 // its transverse halo are staged in shared memory, so each stencil row is
 // read from L2 once per tile instead of once per face row (2.8x fewer for x
-// faces, 4x for y faces at MP7).  128 threads: 32 faces x 4 Gauss lanes, four
-// blocks per SM (smaller blocks than 16 x 4 measured 3-5% faster: a block
-// waiting at the staging barrier holds fewer warps).
+// faces, 4x for y faces at MP7).  128 threads: 32 faces x 4 Gauss lanes
+// (smaller blocks than 16 x 4 measured 3-5% faster: a block waiting at the
+// staging barrier holds fewer warps).
 // ---------------------------------------------------------------------------
 namespace {
 
 constexpr int kFqTX = 8, kFqTY = 4;
+// 96 registers, no spills: five 128-thread blocks per SM measured 8-11%
+// faster than four at 128 registers (six spill and lose it again)
+constexpr int kFqBlocksPerSm = 5;
 
 // TX: faces per tile row; the block has 4 * TX * kFqTY threads.
 template <int DIR, int ORDER, int TX = kFqTX>
@@ -1260,7 +1266,7 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(4 * kFqTX * kFqTY, 512 / (4 * kFqTX * kFqTY))
+__global__ void __launch_bounds__(4 * kFqTX * kFqTY, kFqBlocksPerSm)
     k_face_flux_qs(Grid g, IfaceP in, FluxP out, double* emf, int* nj, double* spd, double gamma,
                    const Ctl* ctl) {
   b_face_flux_qs<DIR, ORDER, kFqTX>(g, in, out, emf, nj, spd, gamma, ctl, blockIdx.x,
@@ -1925,7 +1931,7 @@ __global__ void kb_face_lists(const BatchRec* __restrict__ r, const BatchLearnRe
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(4 * kFqTX * kFqTY, 512 / (4 * kFqTX * kFqTY))
+__global__ void __launch_bounds__(4 * kFqTX * kFqTY, kFqBlocksPerSm)
     kb_face_flux_q(const BatchRec* __restrict__ r, BatchPlan p, int speeds) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
     int local, bx, by;
@@ -1986,7 +1992,7 @@ __global__ void __launch_bounds__(256) kb_fill_ghosts(const BatchRec* __restrict
 }
 
 template <int W>
-__global__ void __launch_bounds__(256) kb_colloc_check(const BatchRec* __restrict__ r,
+__global__ void __launch_bounds__(256, 3) kb_colloc_check(const BatchRec* __restrict__ r,
                                                        BatchPlan p, int theta_mask,
                                                        int live_checks) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
