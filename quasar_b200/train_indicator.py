@@ -89,6 +89,58 @@ def main(argv=None):
     return ind, thr, ev
 
 
+def inference_report(n=2048, order=5, t_develop=0.3, steps=100, snapshots=2, path=None):
+    """The indicator at inference on Orszag-Tang n^2 (periodic, FP64 state).
+    Two solvers advance the plain step bit for bit to t_develop (the shocks
+    have formed); then one runs in learned mode and both take `steps` more
+    steps with the plain run's dt.  Returns the density L1 gap (relative,
+    interior), the recall of the plain run's own limiter activations by the
+    flags (labels at the tolerance the weights were trained with, on
+    `snapshots` evenly spaced plain states of that window) with the fraction
+    of cells flagged, and the mean fraction of faces that took the
+    characteristic path."""
+    from .indicator import learned_face_counts
+    ind, thr = load(path, order)
+    z = np.load(path or default_path(order))
+    tol = float(json.loads(str(z["meta"])).get("tol", 1e-4))
+    solvers = []
+    for _ in range(2):
+        s = _solver(n, order, 0)
+        for name, arr in zip(ics.COMPONENTS, ics.orszag_tang(n, order=order)):
+            s.seed_state(name, arr)
+        t, taken = s.advance_auto(0.0, t_develop, 10 ** 7)
+        solvers.append(s)
+    plain, learned = solvers
+    ind.attach(learned, thr)
+    probe = TroubledCellIndicator(seed=0)
+    probe.set_params(ind.params())
+    ng = ics.nghost(order)
+    universe = 2.0 * (n + 1) * (n + 2 * ng)
+    face_frac = []
+    per = max(1, steps // snapshots)
+    for k in range(steps):
+        if k % per == 0 and k // per < snapshots:
+            probe.collect(plain, tol)
+        dt = plain.cfl_limit()
+        plain.step_unchecked(dt)
+        learned.step_unchecked(dt)
+        fx, fy = learned_face_counts(learned)
+        face_frac.append((fx + fy) / universe)
+    ev = probe.evaluate(thr, holdout=0)
+    sl = (slice(ng, ng + n), slice(ng, ng + n))
+    shape = (n + 2 * ng, n + 2 * ng)
+    rp = plain.state_component_to_host("rho").reshape(shape)[sl]
+    rl = learned.state_component_to_host("rho").reshape(shape)[sl]
+    return {"workload": f"Orszag-Tang {n}^2 MP{order}, periodic: plain to t={t:.4f} "
+                        f"({taken} steps), then {steps} steps plain and learned with the "
+                        "plain run's dt",
+            "rho_l1_vs_plain": float(np.sum(np.abs(rl - rp)) / np.sum(np.abs(rp))),
+            "limiter_recall": ev["recall"], "cells_flagged": ev["flagged"],
+            "label_tol": tol, "labelled_cells": ev["total"], "limiter_positive": ev["positives"],
+            "full_path_face_fraction": float(np.mean(face_frac)),
+            "div_b_max": learned.divergence_b_max()}
+
+
 def default_path(order):
     return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", f"indicator_mp{order}.npz")
 

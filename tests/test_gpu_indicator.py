@@ -119,3 +119,17 @@ def test_collect_train_and_learned_steps():
     l1 = np.sum(np.abs(ra - rb)) / np.sum(np.abs(ra))
     assert l1 <= 1e-3, l1
     assert b.divergence_b_max() <= 1e-12
+
+
+def test_inference_report_on_developed_orszag_tang():
+    """The shipped MP5 indicator at inference on Orszag-Tang 512^2 after the
+    shocks have formed (t = 0.3): the learned step stays within 1e-4 of the
+    plain one in density L1 and its flags catch most of the plain limiter's
+    activations while keeping most faces on the cheap path."""
+    from quasar_b200 import train_indicator
+    r = train_indicator.inference_report(512, 5, t_develop=0.3, steps=60)
+    assert r["limiter_positive"] > 1000
+    assert r["rho_l1_vs_plain"] <= 1e-4
+    assert r["limiter_recall"] >= 0.8
+    assert r["cells_flagged"] < 0.35 and r["full_path_face_fraction"] < 0.35
+    assert r["div_b_max"] <= 1e-10
