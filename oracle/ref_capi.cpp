@@ -15,6 +15,7 @@
 #include "quasar/physics/mhd/mhd_solver.hpp"
 #undef private
 
+#include "quasar/physics/mhd/initial_conditions.hpp"
 #include "quasar/numerics/hlld_core.hpp"
 #include "quasar/numerics/mhd_eigensystem.hpp"
 #include "quasar/numerics/mp_limiter.hpp"
@@ -238,6 +239,58 @@ double qref_mp5(const double* v) {
 double qref_mp7(const double* v) {
   return quasar::numerics::mp7_reconstruct(v[0], v[1], v[2], v[3], v[4],
                                            v[5], v[6]);
+}
+
+// The reference's own deck initial state (build_initial_state,
+// src/physics/mhd/initial_conditions.cpp, over the seed kernels of
+// mhd_initial_conditions.hip).  kind: 0 brio_wu, 1 alfven_wave, 2
+// orszag_tang, 3 blast, 4 rotor, 5 confined_blob.  par[40] in this order:
+// interface, left[8], right[8] (rho, p, vx, vy, vz, bx, by, bz), rho,
+// pressure, b0, total_b0, amplitude, wavenumber, magnetic_velocity_scale,
+// b_uniform[3], center[2], r_in, r0, r1, rho_in, rho_out, p_in, p_out,
+// p_core, p_ambient, rho_ambient, u0, blob_half, magnetic_scale.
+// out8: the 8 padded components.
+int qref_initial_state(int kind, int nx, int ny, double lx, double ly, double ox, double oy,
+                       int ng, double gamma, int order, const double* par,
+                       double* const* out8) {
+  try {
+    quasar::mhd::MhdInitialConditionSpec s;
+    s.kind = static_cast<quasar::mhd::MhdInitialConditionKind>(kind);
+    s.grid = quasar::Grid2D{nx, ny, lx, ly, ox, oy, ng};
+    s.gamma = gamma;
+    s.cylindrical = 0;
+    s.scheme_order = order;
+    int q = 0;
+    s.interface = par[q++];
+    for (int c = 0; c < 8; ++c) s.left[c] = par[q++];
+    for (int c = 0; c < 8; ++c) s.right[c] = par[q++];
+    s.rho = par[q++];
+    s.pressure = par[q++];
+    s.b0 = par[q++];
+    s.total_b0 = par[q++];
+    s.amplitude = par[q++];
+    s.wavenumber = static_cast<std::int64_t>(par[q++]);
+    s.magnetic_velocity_scale = par[q++];
+    for (int c = 0; c < 3; ++c) s.b_uniform[c] = par[q++];
+    for (int c = 0; c < 2; ++c) s.center[c] = par[q++];
+    s.r_in = par[q++];
+    s.r0 = par[q++];
+    s.r1 = par[q++];
+    s.rho_in = par[q++];
+    s.rho_out = par[q++];
+    s.p_in = par[q++];
+    s.p_out = par[q++];
+    s.p_core = par[q++];
+    s.p_ambient = par[q++];
+    s.rho_ambient = par[q++];
+    s.u0 = par[q++];
+    s.blob_half = par[q++];
+    s.magnetic_scale = par[q++];
+    MhdField2D<Real> out{s.grid};
+    quasar::mhd::build_initial_state(s, out, nullptr);
+    for (int c = 0; c < 8; ++c) comp(out, c).copy_to_host(out8[c], s.grid.storage_size());
+    return 0;
+  } catch (const std::exception& e) { return fail(e); }
 }
 
 }  // extern "C"

@@ -187,11 +187,40 @@ class RefLib(_Lib):
         L.qref_residual.argtypes = [ctypes.c_void_p] * 11
         L.qref_divb.argtypes = [ctypes.c_void_p, _dp]
 
-    def solver(self, nx, ny, order, gamma=5.0 / 3.0, cfl=0.4, bc=PERIODIC, lx=1.0, ly=1.0):
-        h = self.lib.qref_create(nx, ny, lx, ly, 0.0, 0.0, order, gamma, cfl, (ctypes.c_int * 4)(*bc))
+    def solver(self, nx, ny, order, gamma=5.0 / 3.0, cfl=0.4, bc=PERIODIC, lx=1.0, ly=1.0,
+               ox=0.0, oy=0.0):
+        h = self.lib.qref_create(nx, ny, lx, ly, ox, oy, order, gamma, cfl, (ctypes.c_int * 4)(*bc))
         if not h:
             raise RuntimeError(self.err())
         return CpuSolver(self, h, nx, ny, order)
+
+    # Parameter order of qref_initial_state (oracle/ref_capi.cpp).
+    IC_PARAMS = (["interface"] + [f"left_{k}" for k in range(8)] +
+                 [f"right_{k}" for k in range(8)] +
+                 ["rho", "pressure", "b0", "total_b0", "amplitude", "wavenumber",
+                  "magnetic_velocity_scale", "bx", "by", "bz", "cx", "cy", "r_in", "r0", "r1",
+                  "rho_in", "rho_out", "p_in", "p_out", "p_core", "p_ambient", "rho_ambient",
+                  "u0", "blob_half", "magnetic_scale"])
+    IC_DEFAULTS = dict(interface=0.5, rho=1.0, pressure=0.1, b0=1.0, total_b0=1.0,
+                       amplitude=1e-6, wavenumber=1.0, magnetic_velocity_scale=1.0, r_in=0.1,
+                       r0=0.1, r1=0.115, rho_in=10.0, rho_out=1.0, p_in=1.0, p_out=0.1,
+                       p_core=10.0, p_ambient=0.1, rho_ambient=1.0, u0=2.0, magnetic_scale=1.0)
+
+    def initial_state(self, kind, nx, ny, lx, ly, ox, oy, ng, gamma, order, **params):
+        """The reference's own build_initial_state (8 padded components)."""
+        vals = dict(self.IC_DEFAULTS, **params)
+        par = np.array([float(vals.get(k, 0.0)) for k in self.IC_PARAMS])
+        n = (nx + 2 * ng) * (ny + 2 * ng)
+        out = [np.zeros(n) for _ in range(8)]
+        L = self.lib
+        L.qref_initial_state.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + \
+            [ctypes.c_double] * 4 + [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_void_p]
+        rc = L.qref_initial_state(kind, nx, ny, lx, ly, ox, oy, ng, gamma, order,
+                                  par.ctypes.data, _ptrs(out))
+        if rc != 0:
+            raise ValueError(self.err())
+        return out
 
 
 def oracle_available():
