@@ -184,6 +184,14 @@ def reference_cpu(case, order, steps, warmup, n=128):
                       f"(cfl_limit + step_unchecked), {cores} OpenMP threads"}
 
 
+def workload_config(a):
+    """The `config` object both arms report."""
+    return {"workload": f"{a.case} {a.n}^2 MP{a.order}+HLLD+upwind CT, SSP-RK3, outflow, "
+                        "gamma 5/3, CFL 0.4 (0.2 effective)",
+            "n": a.n, "order": a.order, "parallelism": f"replicas x{WORLD}",
+            "l2": "state 1 GB+ per register, larger than L2"}
+
+
 def run_reference_arm(a):
     if RANK != 0:
         return
@@ -193,8 +201,8 @@ def run_reference_arm(a):
             "value": cpu["value"], "unit": "zone-updates/s", "n_gpus": a.gpus, "steps": steps,
             "warmup": warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{a.case} MP{a.order}+HLLD+CT SSP-RK3 outflow", "n": a.n,
-                       "sample_n": 128},
+            "config": dict(workload_config(a), sample_n=128,
+                           sample="each step a 128^2 instance of the workload on the host cores"),
             "cpu_baseline": cpu,
             "e2e": {"value": cpu["value"], "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -420,10 +428,7 @@ def main():
                 "unit": "zone-updates/s", "n_gpus": WORLD, "steps": a.steps, "warmup": a.warmup,
                 "ms_per_step": t_ms / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": f"{a.case} {a.n}^2 MP{a.order}+HLLD+upwind CT, SSP-RK3, "
-                                       "outflow, gamma 5/3, CFL 0.4 (0.2 effective)",
-                           "n": a.n, "order": a.order, "parallelism": f"replicas x{WORLD}",
-                           "l2": "state 1 GB+ per register, larger than L2"},
+                "config": workload_config(a),
                 "gpu_launches": LAUNCHES_PER_STEP * a.steps,
                 "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
                 "learned": learned, "batched": batched, "batched_learned": combined}
