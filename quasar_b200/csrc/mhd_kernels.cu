@@ -1094,36 +1094,44 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// MP5/MP7 face flux with one lane per Gauss point: a group of four lanes owns
-// a face.  Each lane recovers its point state and solves its Riemann problem;
-// the group votes on admissibility, gathers the point fluxes in node order for
-// the Gauss sum, and splits the stores.  Same arithmetic as k_face_flux (node
-// order of every sum kept).  The interface states of an 8 x 4 face tile and
-// its transverse halo are staged in shared memory, so each stencil row is
-// read from L2 once per tile instead of once per face row (2.8x fewer for x
-// faces, 4x for y faces at MP7).  128 threads: 32 faces x 4 Gauss lanes
-// (smaller blocks than 16 x 4 measured 3-5% faster: a block waiting at the
-// staging barrier holds fewer warps).
+// MP5/MP7 face flux with one lane per Gauss point: a group of Q lanes owns a
+// face (Q = 3 at MP5, 4 at MP7).  Each lane recovers its point state and
+// solves its Riemann problem; the group votes on admissibility, gathers the
+// point fluxes in node order for the Gauss sum, and splits the stores.  Same
+// arithmetic as k_face_flux (node order of every sum kept).  The interface
+// states of a face tile (8 x 4 at MP7, 8 x 5 at MP5) and its transverse halo
+// are staged in shared memory, so each stencil row is read from L2 once per
+// tile instead of once per face row (2.8x fewer for x faces, 4x for y faces
+// at MP7).  128 threads (smaller blocks than 16 x 4 measured 3-5% faster at
+// MP7: a block waiting at the staging barrier holds fewer warps).
 // ---------------------------------------------------------------------------
 namespace {
 
 constexpr int kFqTX = 8, kFqTY = 4;
+// One lane per Gauss point: groups of 4 lanes (MP7, 8 faces per warp, 8 x 4
+// face tiles) or 3 lanes (MP5, 10 faces per warp with two lanes idle, 8 x 5
+// tiles); four warps per block either way.
+constexpr int kFqThreads = 4 * kFqTX * kFqTY;
+template <int ORDER>
+constexpr int fq_ty() { return ORDER == 5 ? 5 : 4; }
 // 96 registers, no spills: five 128-thread blocks per SM measured 8-11%
 // faster than four at 128 registers (six spill and lose it again)
 constexpr int kFqBlocksPerSm = 5;
 
-// TX: faces per tile row; the block has 4 * TX * kFqTY threads.
+// TX: faces per tile row; the block is four warps of 32 / Q groups each.
 template <int DIR, int ORDER, int TX = kFqTX>
 __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, const FluxP& out,
                                                double* emf, int* nj, double* spd, double gamma,
                                                const Ctl* ctl, int bx, int by) {
   constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
-  constexpr int TR = DIR == 0 ? kFqTY + 2 * H : kFqTY;   // tile rows (j)
-  constexpr int TC = DIR == 0 ? TX : TX + 2 * H;         // tile columns (i)
+  constexpr int FPW = 32 / Q, TY = fq_ty<ORDER>();         // faces per warp, tile rows
+  static_assert(4 * FPW == TX * TY, "four warps cover the face tile");
+  constexpr int TR = DIR == 0 ? TY + 2 * H : TY;          // tile rows (j)
+  constexpr int TC = DIR == 0 ? TX : TX + 2 * H;          // tile columns (i)
   __shared__ double tile[16][TR][TC];
   __shared__ unsigned char same[TR][TC];  // staged and L == R in every component
   if (ctl->status) return;  // uniform over the block
-  const int i0 = bx * TX, j0 = by * kFqTY;
+  const int i0 = bx * TX, j0 = by * TY;
   const bool perx = g.bc[0] == 0 && g.bc[1] == 0, pery = g.bc[2] == 0 && g.bc[3] == 0;
   for (int e = threadIdx.x; e < TR * TC; e += blockDim.x) {
     const int row = e / TC, col = e - row * TC;
@@ -1154,11 +1162,14 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
   }
   __syncthreads();
   constexpr bool kLF = false;
-  const int lane = threadIdx.x & 3, grp = threadIdx.x >> 2;
-  const unsigned gmask = 0xFu << (threadIdx.x & 28);
-  const int fx = grp % TX, fy = grp / TX;
+  const int wl = threadIdx.x & 31;
+  if (wl >= FPW * Q) return;  // the lanes no group uses (MP5)
+  const int lane = wl % Q, base = wl - lane;
+  const unsigned gmask = ((1u << Q) - 1u) << base;
+  const int face = (threadIdx.x >> 5) * FPW + wl / Q;
+  const int fx = face % TX, fy = face / TX;
   const int i = i0 + fx, j = j0 + fy;
-  if (i > g.nx || j > g.ny) return;  // whole four-lane groups leave together
+  if (i > g.nx || j > g.ny) return;  // whole groups leave together
   const long long k = g.idx(i, j);
   const double h = DIR == 0 ? g.dx : g.dy;
   // tile coordinates of stencil tap t (t = H is the face itself)
@@ -1166,7 +1177,7 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
   auto tcl = [&](int t) { return DIR == 0 ? fx : fx + t; };
   St l{}, r{};
   bool ok = true;
-  if (lane < Q) {
+  {
     double w[N];
 #pragma unroll
     for (int t = 0; t < N; ++t) w[t] = point_w<ORDER>(lane, t);
@@ -1191,7 +1202,7 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
     return St{tile[o][rr][cc],     tile[o + 1][rr][cc], tile[o + 2][rr][cc], tile[o + 3][rr][cc],
               tile[o + 4][rr][cc], tile[o + 5][rr][cc], tile[o + 6][rr][cc], tile[o + 7][rr][cc]};
   };
-  const unsigned bad = (__ballot_sync(gmask, !ok) >> (threadIdx.x & 28)) & 0xFu;
+  const unsigned bad = (__ballot_sync(gmask, !ok) >> base) & ((1u << Q) - 1u);
   const bool group_ok = bad == 0;
   const int first_bad = bad ? __ffs(bad) - 1 : Q;
   double rate = 0.0;
@@ -1199,7 +1210,7 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
     if (lane == 0) rate = face_rate<DIR, ORDER>(centre(true), centre(false), gamma, h);
     if (lane < first_bad) rate = fmax(rate, face_rate<DIR, ORDER>(l, r, gamma, h));
   }
-  const bool solve = group_ok ? lane < Q : lane == 0;
+  const bool solve = group_ok || lane == 0;
   if (!group_ok) {
     l = centre(true);
     r = centre(false);
@@ -1216,34 +1227,33 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
     if (group_ok) {
       double sq[Q];
 #pragma unroll
-      for (int q = 0; q < Q; ++q) sq[q] = __shfl_sync(gmask, fv[c], q, 4);
+      for (int q = 0; q < Q; ++q) sq[q] = __shfl_sync(gmask, fv[c], base + q);
       res[c] = gauss_avg<ORDER>(sq);
     } else {
-      res[c] = __shfl_sync(gmask, fv[c], 0, 4);
+      res[c] = __shfl_sync(gmask, fv[c], base);
     }
   }
-  const double lo = lane == 0 ? res[0] : lane == 1 ? res[1] : lane == 2 ? res[2] : res[3];
-  const double hi = lane == 0 ? res[4] : lane == 1 ? res[5] : lane == 2 ? res[6] : res[7];
-  double* const flo = lane == 0 ? out.f[0] : lane == 1 ? out.f[1] : lane == 2 ? out.f[2] : out.f[3];
-  double* const fhi = lane == 0 ? out.f[4] : lane == 1 ? out.f[5] : lane == 2 ? out.f[6] : out.f[7];
   // out, emf and nj may each be absent (the per-kernel launch interface
-  // asks for fluxes or for the CT face tables alone)
+  // asks for fluxes or for the CT face tables alone); the stores are split
+  // over the group (component c by lane c mod Q)
   if (out.f[0]) {
-    flo[k] = lo;
-    fhi[k] = hi;
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (c % Q == lane) out.f[c][k] = res[c];
   }
   if (lane == 0 && emf) emf[k] = DIR == 0 ? -res[6] : res[5];
   if (spd) {
-    rate = fmax(rate, __shfl_xor_sync(gmask, rate, 1, 4));
-    rate = fmax(rate, __shfl_xor_sync(gmask, rate, 2, 4));
-    if (lane == 0) spd[k] = rate;
+    double m = rate;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) m = fmax(m, __shfl_sync(gmask, rate, base + q));
+    if (lane == 0) spd[k] = m;
   }
   if (!nj) return;  // uniform over the block
   // no-jump proof over the 2H+1 transverse taps (mapped like every CT table
   // read), split across the group.  A tap whose mapped face is the one staged
   // in its tile slot reads the staged comparison; the others read memory.
   int proof = 1;
-  for (int off = lane - H; off <= H; off += 4) {
+  for (int off = lane - H; off <= H; off += Q) {
     const int mi = face_index(DIR == 0 ? i : i + off, g.nx, g.bc[0], g.bc[1]);
     const int mj = face_index(DIR == 0 ? j + off : j, g.ny, g.bc[2], g.bc[3]);
     const int ti = DIR == 0 ? ((i == g.nx && perx) ? 0 : i) : i + off;
@@ -1261,12 +1271,12 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
     for (int c = 0; c < 8; ++c)
       if (!(in.L[c][km] == in.R[c][km])) proof = 0;
   }
-  const unsigned nproof = (__ballot_sync(gmask, proof == 0) >> (threadIdx.x & 28)) & 0xFu;
+  const unsigned nproof = (__ballot_sync(gmask, proof == 0) >> base) & ((1u << Q) - 1u);
   if (lane == 0) nj[k] = nproof == 0 ? 1 : 0;
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(4 * kFqTX * kFqTY, kFqBlocksPerSm)
+__global__ void __launch_bounds__(kFqThreads, kFqBlocksPerSm)
     k_face_flux_qs(Grid g, IfaceP in, FluxP out, double* emf, int* nj, double* spd, double gamma,
                    const Ctl* ctl) {
   b_face_flux_qs<DIR, ORDER, kFqTX>(g, in, out, emf, nj, spd, gamma, ctl, blockIdx.x,
@@ -1931,7 +1941,7 @@ __global__ void kb_face_lists(const BatchRec* __restrict__ r, const BatchLearnRe
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(4 * kFqTX * kFqTY, kFqBlocksPerSm)
+__global__ void __launch_bounds__(kFqThreads, kFqBlocksPerSm)
     kb_face_flux_q(const BatchRec* __restrict__ r, BatchPlan p, int speeds) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
     int local, bx, by;
@@ -2092,8 +2102,9 @@ template <int DIR, int ORDER>
 static void flux_launch(const StageArgs& a, bool speeds, cudaStream_t s) {
   const Grid& g = a.g;
   if (ORDER == 5 || ORDER == 7) {
-    const dim3 grid(cdiv(g.nx + 1, kFqTX), cdiv(g.ny + 1, kFqTY));
-    k_face_flux_qs<DIR, ORDER == 5 ? 5 : 7><<<grid, 4 * kFqTX * kFqTY, 0, s>>>(
+    constexpr int O = ORDER == 5 ? 5 : 7;
+    const dim3 grid(cdiv(g.nx + 1, kFqTX), cdiv(g.ny + 1, fq_ty<O>()));
+    k_face_flux_qs<DIR, O><<<grid, kFqThreads, 0, s>>>(
         g, DIR == 0 ? a.ix : a.iy, DIR == 0 ? a.fx : a.fy, DIR == 0 ? a.xemf : a.yemf,
         DIR == 0 ? a.xnj : a.ynj, speeds ? (DIR == 0 ? a.xspd : a.yspd) : nullptr, a.gamma, a.ctl);
     return;
@@ -2211,7 +2222,7 @@ void batch_cell_configure() {
 int batch_phase_threads(int phase) {
   switch (phase) {
     case kBpRecon0: case kBpRecon1: case kBpCorner: return 128;
-    case kBpFlux: return 4 * kFqTX * kFqTY;
+    case kBpFlux: return kFqThreads;
     default: return 256;
   }
 }
@@ -2230,7 +2241,7 @@ int batch_phase_max_ctas_per_sm(int phase, int order) {
       return o7 ? max_ctas(kb_reconstruct<1, 7>, 128, kReconSmem)
                 : max_ctas(kb_reconstruct<1, 5>, 128, kReconSmem);
     case kBpFlux: {
-      constexpr int t = 4 * kFqTX * kFqTY;
+      constexpr int t = kFqThreads;
       return o7 ? max_ctas(kb_face_flux_q<0, 7>, t, 0) : max_ctas(kb_face_flux_q<0, 5>, t, 0);
     }
     case kBpCell:
@@ -2273,11 +2284,11 @@ void launch_batch_face_flux(const BatchRec* r, const BatchPlan& p, int dir, int 
                             bool speeds, cudaStream_t s) {
   const int sp = speeds ? 1 : 0;
   if (order == 7) {
-    if (dir == 0) kb_face_flux_q<0, 7><<<pgrid(p), 4 * kFqTX * kFqTY, 0, s>>>(r, p, sp);
-    else kb_face_flux_q<1, 7><<<pgrid(p), 4 * kFqTX * kFqTY, 0, s>>>(r, p, sp);
+    if (dir == 0) kb_face_flux_q<0, 7><<<pgrid(p), kFqThreads, 0, s>>>(r, p, sp);
+    else kb_face_flux_q<1, 7><<<pgrid(p), kFqThreads, 0, s>>>(r, p, sp);
   } else {
-    if (dir == 0) kb_face_flux_q<0, 5><<<pgrid(p), 4 * kFqTX * kFqTY, 0, s>>>(r, p, sp);
-    else kb_face_flux_q<1, 5><<<pgrid(p), 4 * kFqTX * kFqTY, 0, s>>>(r, p, sp);
+    if (dir == 0) kb_face_flux_q<0, 5><<<pgrid(p), kFqThreads, 0, s>>>(r, p, sp);
+    else kb_face_flux_q<1, 5><<<pgrid(p), kFqThreads, 0, s>>>(r, p, sp);
   }
 }
 
