@@ -21,8 +21,8 @@
  *     MP7, 3 for MP5, 2 for MUSCL; order 1 (the positivity retry) runs on
  *     any of them;
  *   - status codes and qmhd_last_error() as in quasar_mhd.h; a cylindrical
- *     grid, an active background field, a rate-only reconstruction or a
- *     partial face ownership is QMHD_INVALID_ARGUMENT (out of scope).
+ *     grid, an active background field or a partial face ownership is
+ *     QMHD_INVALID_ARGUMENT (out of scope).
  *
  * Reductions write into `scratch`: caller-owned device memory of at least
  * QMHD_LAUNCH_SCRATCH_BYTES, 8-byte aligned, whose content need not be
@@ -84,7 +84,9 @@ typedef struct qmhd_cfl_rate {
 /* launch_mhd_reconstruct (kernels.hpp:162-166): left/right conserved states
  * of every face normal to dir (0 x, 1 y) for scheme_order 1, 2, 5 or 7.
  * cell_bx, cell_by: caller scratch (padded arrays) that receives the
- * face-to-cell collocated field of u, which the reconstruction reads. */
+ * face-to-cell collocated field of u, which the reconstruction reads.
+ * rate_only (the CFL path's flag) gives the same states, as in the reference,
+ * where it only picks an admissibility predicate that forwards to the other. */
 int qmhd_launch_reconstruct(const qmhd_grid* grid, const qmhd_field* u, double* cell_bx,
                             double* cell_by, int dir, const qmhd_iface* out,
                             int scheme_order, const int flags[4], double gamma, void* stream,

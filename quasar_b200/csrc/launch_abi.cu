@@ -174,7 +174,10 @@ int qmhd_launch_reconstruct(const qmhd_grid* grid, const qmhd_field* u, double* 
     check_order(fn, g, scheme_order);
     check_dir(fn, dir);
     check_gamma(fn, gamma);
-    if (rate_only) bad(fn, "rate-only reconstruction is not supported");
+    // rate_only only selects reconstructed_rate_state_admissible, which
+    // forwards to reconstructed_state_admissible (mhd_reconstruct.hip:449-452,
+    // 654-659): the same reconstruction either way
+    (void)rate_only;
     if (!cell_bx || !cell_by) bad(fn, "null collocation scratch");
     const StateP st = state_of(fn, u, cell_bx, cell_by);
     const IfaceP io = iface_of(fn, out);

@@ -88,7 +88,9 @@ def test_launch_interface_rejects_bad_arguments_before_any_launch():
     with pytest.raises(ValueError, match="cylindrical"):
         _native.check(lib.qmhd_launch_flux_difference(ctypes.byref(g), ctypes.byref(u), 0,
                                                       ctypes.byref(u), None, 1))
-    with pytest.raises(ValueError, match="rate-only"):
+    # rate_only is accepted (same states as the reference): the call gets as
+    # far as the scratch check
+    with pytest.raises(ValueError, match="collocation scratch"):
         _native.check(lib.qmhd_launch_reconstruct(ctypes.byref(g), ctypes.byref(u), None, None, 0,
                                                   ctypes.byref(iface), 7, per, 5 / 3, None, 1))
     with pytest.raises(ValueError, match="ownership"):
@@ -116,3 +118,22 @@ def test_python_config_validation_matches_reference_errors():
     cfg.boundary.field = list(cfg.boundary.fluid)
     c = mhd._native_config(cfg)  # the periodic pairing is checked natively
     assert list(c.boundary) == [0, 1, 0, 0]
+
+
+def test_seam_build_loads_and_reports_a_missing_device_as_the_reference_does():
+    """oracle/_ref/libquasar_mhd_seam.so (the reference's own MhdSolver2D
+    linked over this library's launch interface) loads, binds every
+    kernels.hpp entry point at link time, and without a GPU its solver
+    constructor fails with the reference's DeviceError text instead of
+    crashing."""
+    import pytest
+    import torch
+    import mhd_cases as M
+    so = os.path.join(ROOT, "oracle", "_ref", "libquasar_mhd_seam.so")
+    if not os.path.exists(so):
+        pytest.skip("seam build absent (oracle/build_seam.sh)")
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: the GPU tests cover the seam")
+    lib = M.RefLib(so)
+    with pytest.raises(RuntimeError, match="device error"):
+        lib.solver(16, 16, 5)

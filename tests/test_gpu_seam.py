@@ -1,0 +1,153 @@
+"""The reference's own, unmodified MhdSolver2D (mhd_solver.cpp with its
+numerics registry) running on this project's kernels through the per-kernel
+seam: oracle/seam/mhd_kernels_b200.cpp defines every kernels.hpp declaration
+over include/quasar_mhd_launch.h, oracle/build_seam.sh links the result into
+oracle/_ref/libquasar_mhd_seam.so with the same qref_* driver as the CPU
+build.  The reference's host sequencing, interface cache, CFL path
+(rate-only reconstruction), positivity controller, solenoidality preflight
+and diagnostics all run unchanged; only the kernels are this project's.
+
+Checks: against the reference built for the CPU (per-step state within 1e-10
+relative L1 per physical group, dt within 1e-12 relative, same diagnostics
+and the same error), and against this project's fused solver step (bit for
+bit: the seam launches the same kernels in the reference's order)."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import mhd_cases as M
+
+pytestmark = pytest.mark.gpu
+
+SEAM_SO = os.path.join(M.ROOT, "oracle", "_ref", "libquasar_mhd_seam.so")
+ORDER_NAME = {2: "muscl_minmod", 5: "mp5", 7: "mp7"}
+BC_NAME = {0: "periodic", 1: "outflow", 2: "wall"}
+STEP_TOL = 1e-10
+DT_TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def seam():
+    if not os.path.exists(SEAM_SO):
+        pytest.skip("seam build absent (oracle/build_seam.sh)")
+    return M.RefLib(SEAM_SO)
+
+
+def totals(lib, s):
+    lib.lib.qref_totals.argtypes = [ctypes.c_void_p, M._dp, M._dp]
+    m, e = ctypes.c_double(), ctypes.c_double()
+    assert lib.lib.qref_totals(s.h, m, e) == 0, lib.err()
+    return m.value, e.value
+
+
+def divb(lib, s):
+    d = ctypes.c_double()
+    assert lib.lib.qref_divb(s.h, d) == 0, lib.err()
+    return d.value
+
+
+def fused(nx, ny, order, bc, lx=1.0, ly=1.0, ox=0.0, oy=0.0):
+    from quasar_b200 import mhd
+    cfg = mhd.MhdConfig()
+    cfg.grid = mhd.Grid2D(nx, ny, lx, ly, ox, oy)
+    cfg.reconstruction = ORDER_NAME[order]
+    cfg.boundary = mhd.MhdBoundarySpec([BC_NAME[b] for b in bc], [BC_NAME[b] for b in bc])
+    return mhd.MhdSolver2D(cfg)
+
+
+def pulse(nx, ny, order, bc, lx, ly, ox, oy):
+    """Pressure pulse off centre, field tangential to every wall."""
+    from quasar_b200 import ics
+    ng = M.nghost(order)
+    X, Y = np.meshgrid(ics._centres(nx, ng, lx, ox), ics._centres(ny, ng, ly, oy), indexing="xy")
+    r = np.hypot(X - 0.3, Y - 0.55)
+    p = np.where(r < 0.2, 5.0, 0.5)
+    rho = 1.0 + 0.2 * np.exp(-8.0 * r * r)
+    zero = np.zeros_like(X)
+    by = zero + (0.6 if bc[2] != 2 and bc[3] != 2 else 0.0)
+    return ics._assemble(rho, 0.1 * np.cos(2.0 * Y), zero, zero, p, zero, by, zero + 0.3, 5.0 / 3.0)
+
+
+CASES = {
+    "ot32_mp5": dict(n=(32, 32), order=5, bc=M.PERIODIC, ic=lambda: M.orszag_tang(32, order=5)),
+    "rotor32_mp7": dict(n=(32, 32), order=7, bc=M.PERIODIC, ic=lambda: M.rotor(32, order=7)),
+    "blast32_mp7": dict(n=(32, 32), order=7, bc=M.PERIODIC, ic=lambda: M.blast(32, order=7)),
+    "pulse40x24_mp7_walls": dict(n=(40, 24), order=7, bc=(2, 2, 2, 2), dom=(2.0, 0.75, -1.0, 0.25)),
+    "pulse40x24_mp5_mixed": dict(n=(40, 24), order=5, bc=(1, 2, 0, 0), dom=(2.0, 0.75, -1.0, 0.25)),
+    "ot24_muscl": dict(n=(24, 24), order=2, bc=M.PERIODIC, ic=lambda: M.orszag_tang(24, order=2)),
+}
+
+
+def setup(case):
+    c = CASES[case]
+    nx, ny = c["n"]
+    lx, ly, ox, oy = c.get("dom", (1.0, 1.0, 0.0, 0.0))
+    ic = c["ic"]() if "ic" in c else pulse(nx, ny, c["order"], c["bc"], lx, ly, ox, oy)
+    return nx, ny, c["order"], c["bc"], (lx, ly, ox, oy), ic
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_reference_solver_on_seam_matches_cpu_reference(seam, ref, case):
+    nx, ny, order, bc, (lx, ly, ox, oy), ic = setup(case)
+    ng = M.nghost(order)
+    g = seam.solver(nx, ny, order, bc=bc, lx=lx, ly=ly, ox=ox, oy=oy)
+    c = ref.solver(nx, ny, order, bc=bc, lx=lx, ly=ly, ox=ox, oy=oy)
+    g.seed(ic)
+    c.seed(ic)
+    for k in range(5):
+        dt_c, dt_g = c.cfl(), g.cfl()
+        assert abs(dt_g - dt_c) <= DT_TOL * dt_c, (k, dt_g, dt_c)
+        c.step(dt_c)
+        g.step(dt_c)
+        assert g.substeps() == c.substeps()
+        err = M.state_rel_l1(g.read(), c.read(), ng, nx, ny)
+        assert err <= STEP_TOL, (k, err)
+    assert divb(seam, g) <= 1e-12 and divb(ref, c) <= 1e-12
+    (mg, eg), (mc, ec) = totals(seam, g), totals(ref, c)
+    assert abs(mg - mc) <= 1e-12 * abs(mc)
+    assert abs(eg - ec) <= 1e-12 * abs(ec)
+
+
+@pytest.mark.parametrize("case", ["ot32_mp5", "rotor32_mp7", "pulse40x24_mp7_walls", "ot24_muscl"])
+def test_reference_solver_on_seam_equals_fused_step(seam, case):
+    """The reference's driver over the seam and this project's fused step
+    launch the same kernels: dt and state agree bit for bit."""
+    nx, ny, order, bc, (lx, ly, ox, oy), ic = setup(case)
+    g = seam.solver(nx, ny, order, bc=bc, lx=lx, ly=ly, ox=ox, oy=oy)
+    f = fused(nx, ny, order, bc, lx, ly, ox, oy)
+    g.seed(ic)
+    for name, a in zip(M.COMPONENTS, ic):
+        f.seed_state(name, a)
+    shape = g.shape
+    for k in range(4):
+        dt = g.cfl()
+        assert f.cfl_limit() == dt, k
+        g.step(dt)
+        f.step_unchecked(dt)
+        mine = [f.state_component_to_host(cn).reshape(shape) for cn in M.COMPONENTS]
+        theirs = g.read()
+        for c, (a, b) in enumerate(zip(mine, theirs)):
+            np.testing.assert_array_equal(M._evolved(a, c, g.ng, nx, ny),
+                                          M._evolved(b, c, g.ng, nx, ny),
+                                          err_msg=f"step {k} {M.COMPONENTS[c]}")
+
+
+def test_seam_raises_the_reference_preflight_error(seam, ref):
+    """A face field that is not discretely solenoidal: the reference's
+    preflight (its divb-relative launch, here this project's kernel) refuses
+    the step with the same message on both builds."""
+    nx = ny = 32
+    ic = list(M.orszag_tang(32, order=5))
+    rng = np.random.default_rng(3)
+    ic[5] = ic[5] + 1e-3 * rng.standard_normal(ic[5].shape)
+    msgs = []
+    for lib in (seam, ref):
+        s = lib.solver(nx, ny, 5)
+        with pytest.raises(RuntimeError) as e:
+            s.seed(ic)
+            s.step(1e-4)
+        msgs.append(str(e.value))
+    assert "divergence-free" in msgs[0]
+    assert msgs[0] == msgs[1]
