@@ -468,12 +468,15 @@ void MhdSolver2D::controller(double dt, double theta, bool anchor) {
     bool low_interval = false, high = true, pending = true;
     int retries = 0, attempts = 1;
     last_substeps_ = 0;
-    auto no_progress = [&](const char* what) {
+    // message of mhd_solver.cpp:1009-1020, counters at the point of failure
+    auto no_progress = [&](const char* what, double th) {
       low_order_ = 0;
       std::ostringstream m;
       m.precision(17);
       m << "MhdSolver2D: " << what << " cannot advance time (trial=" << trial
-        << ", remaining=" << remaining << ", theta=" << theta << ")";
+        << ", remaining=" << remaining << ", theta=" << th
+        << ", low_order=" << (low_interval ? "true" : "false") << ", retries=" << retries
+        << ", accepted_substeps=" << last_substeps_ << ", attempts=" << attempts << ")";
       return std::runtime_error(m.str());
     };
     while (remaining > 0.0) {
@@ -486,14 +489,15 @@ void MhdSolver2D::controller(double dt, double theta, bool anchor) {
         bool switched = false;
         if (high) {
           const Ctl c = read_ctl();
-          if (from_bits(c.anchor_theta) >= 1.0) {
+          const double anchor_theta = from_bits(c.anchor_theta);
+          if (anchor_theta >= 1.0) {
             anchor = true;
             low_interval = true;
             low_order_ = 1;
             anchor_mode_ = 1;
             trial = std::min(trial, cfl_limit_for(1));
             if (!(trial > 0.0) || !std::isfinite(trial) || !(remaining - trial < remaining))
-              throw no_progress("low-order CFL substep");
+              throw no_progress("low-order CFL substep", anchor_theta);
             switched = true;
           }
         }
@@ -501,7 +505,7 @@ void MhdSolver2D::controller(double dt, double theta, bool anchor) {
           trial *= std::max(0.05, std::min(0.8, 0.8 * theta));
           low_order_ = low_interval ? 1 : 0;
           if (!(trial > 0.0) || !std::isfinite(trial) || !(remaining - trial < remaining))
-            throw no_progress("positive conservative substep");
+            throw no_progress("positive conservative substep", theta);
         }
       }
       if (++attempts > 100000)

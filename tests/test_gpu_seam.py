@@ -151,3 +151,65 @@ def test_seam_raises_the_reference_preflight_error(seam, ref):
         msgs.append(str(e.value))
     assert "divergence-free" in msgs[0]
     assert msgs[0] == msgs[1]
+
+
+def test_reference_positivity_controller_on_seam(seam, ref):
+    """A step three times the CFL limit on a blast with a thousandfold core
+    energy: the reference's controller rolls back and retries with smaller
+    substeps and the order-1 anchor, calling this project's admissible-
+    fraction and order-1 kernels.  Same substep count and state as the
+    reference's CPU build; same as this project's fused controller."""
+    n, order = 16, 5
+    ic = list(M.blast(n, order=order))
+    ic[4] = np.where(ic[4] > 100, ic[4] * 1e3, ic[4])
+    g = seam.solver(n, n, order, bc=M.OUTFLOW)
+    c = ref.solver(n, n, order, bc=M.OUTFLOW)
+    f = fused(n, n, order, M.OUTFLOW)
+    g.seed(ic)
+    c.seed(ic)
+    for name, a in zip(M.COMPONENTS, ic):
+        f.seed_state(name, a)
+    dt = 3.0 * c.cfl()
+    c.step(dt)
+    g.step(dt)
+    f.step_unchecked(dt)
+    assert g.substeps() == c.substeps() == f.last_positivity_substeps() >= 2
+    mine = [f.state_component_to_host(cn).reshape(g.shape) for cn in M.COMPONENTS]
+    assert M.state_rel_l1(g.read(), c.read(), g.ng, n, n) <= STEP_TOL
+    assert M.state_rel_l1(mine, g.read(), g.ng, n, n) <= STEP_TOL
+
+
+def test_exhausted_controller_matches_reference_driver(seam):
+    """Blast 128^2 MP5 with outflow sides under the automatic dt: this
+    project's fused solver and the reference's driver over the seam take the
+    same dt and substeps and stay bit-identical for 60 steps (one of them
+    with a positivity retry); on step 61 the controller runs out of
+    representable time progress in both, with the reference's message and
+    the same counters."""
+    n, order = 128, 5
+    ic = list(M.blast(n, order=order))
+    g = seam.solver(n, n, order, bc=M.OUTFLOW)
+    f = fused(n, n, order, M.OUTFLOW)
+    g.seed(ic)
+    for name, a in zip(M.COMPONENTS, ic):
+        f.seed_state(name, a)
+    retried = 0
+    for k in range(61):
+        dt = g.cfl()
+        assert f.cfl_limit() == dt, k
+        g.step(dt)
+        f.step_unchecked(dt)
+        assert g.substeps() == f.last_positivity_substeps(), k
+        retried += g.substeps() > 1
+    assert retried >= 1
+    mine = [f.state_component_to_host(cn).reshape(g.shape) for cn in M.COMPONENTS]
+    for c, (a, b) in enumerate(zip(mine, g.read())):
+        np.testing.assert_array_equal(M._evolved(a, c, g.ng, n, n), M._evolved(b, c, g.ng, n, n))
+    dt = g.cfl()
+    assert f.cfl_limit() == dt
+    with pytest.raises(RuntimeError) as eg:
+        g.step(dt)
+    with pytest.raises(RuntimeError) as ef:
+        f.step_unchecked(dt)
+    assert "cannot advance time" in str(eg.value)
+    assert str(ef.value) == str(eg.value)
