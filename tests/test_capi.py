@@ -137,3 +137,22 @@ def test_seam_build_loads_and_reports_a_missing_device_as_the_reference_does():
     lib = M.RefLib(so)
     with pytest.raises(RuntimeError, match="device error"):
         lib.solver(16, 16, 5)
+
+
+def test_seam_and_cpu_reference_builds_load_into_one_process():
+    """Both builds carry the reference's registry singletons and register the
+    same factory names at load time.  The seam library keeps its copies
+    local, so loading it after the CPU build (as the GPU tests do) must not
+    end the process with a duplicate-registration error.  Run in a child
+    process, since that error aborts."""
+    import subprocess
+    import sys
+    import pytest
+    seam = os.path.join(ROOT, "oracle", "_ref", "libquasar_mhd_seam.so")
+    cpu = os.path.join(ROOT, "oracle", "_ref", "libquasar_mhd_ref.so")
+    if not (os.path.exists(seam) and os.path.exists(cpu)):
+        pytest.skip("reference builds absent (oracle/build_ref.sh, oracle/build_seam.sh)")
+    code = ("import ctypes; ctypes.CDLL(%r); ctypes.CDLL(%r); print('both loaded')" % (cpu, seam))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "both loaded" in r.stdout
