@@ -1376,12 +1376,13 @@ __global__ void __launch_bounds__(128) k_cell_emf(Grid g, StateP u, double* cell
   }
 }
 
-// Tiled form of k_cell_emf for MP5/MP7: a 32x8 tile of cells and its
+// Tiled form of k_cell_emf for MP5/MP7: a 16x16 tile of cells and its
 // H-wide halo are staged in shared memory once; for each x-node the
 // x-recovered rows of the tile (all 8 components) are formed once in shared
 // memory and every cell then recovers its y-nodes from them.  Same sums in
-// the same order as k_cell_emf.
-constexpr int kCellTX = 32, kCellTY = 8;
+// the same order as k_cell_emf.  A square tile recovers fewer halo rows per
+// cell than 32x8 (22/16 against 14/8 at MP7).
+constexpr int kCellTX = 16, kCellTY = 16;
 
 template <int ORDER>
 constexpr int cell_smem_doubles() {

@@ -183,7 +183,7 @@ __host__ __device__ inline void batch_tiles(int phase, const Grid& g, int* tx, i
     case kBpRecon1: *tx = cd(g.nx + 2 * g.ng, 32); *ty = cd(g.ny + 1, 4); break;
     // face tiles of 8 x 4 (MP7, 4 ghosts) or 8 x 5 (MP5, 3 ghosts) faces
     case kBpFlux: *tx = cd(g.nx + 1, 8); *ty = cd(g.ny + 1, g.ng == 3 ? 5 : 4); break;
-    case kBpCell: *tx = cd(g.nx + 1, 32); *ty = cd(g.ny + 1, 8); break;
+    case kBpCell: *tx = cd(g.nx + 1, 16); *ty = cd(g.ny + 1, 16); break;  // kCellTX x kCellTY
     case kBpCorner: *tx = cd(g.nx + 1, 32); *ty = cd(g.ny + 1, 4); break;
     case kBpUpdate: *tx = cd(g.nx + 1, 32); *ty = cd(g.ny + 1, 8); break;
     case kBpColloc: *tx = cd(g.nx + 2 * g.ng, 32); *ty = cd(g.ny + 2 * g.ng, 8); break;
