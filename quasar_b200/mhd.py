@@ -47,11 +47,51 @@ class Grid2D:
         return (self.nx + 2 * self.nghost) * (self.ny + 2 * self.nghost)
 
 
+def _side(side: int) -> int:
+    # pybind11 maps the binding's std::out_of_range("side") to IndexError
+    if not 0 <= int(side) <= 3:
+        raise IndexError("side")
+    return int(side)
+
+
 @dataclass
 class MhdBoundarySpec:
-    """boundary/mhd_boundary.hpp: per-side registry names, [x_lo,x_hi,y_lo,y_hi]."""
+    """boundary/mhd_boundary.hpp: per-side registry names, [x_lo,x_hi,y_lo,y_hi],
+    with the setters and getters of bind_mhd.cpp:503-545."""
     fluid: List[str] = field(default_factory=lambda: ["periodic"] * 4)
     field: List[str] = field(default_factory=lambda: ["periodic"] * 4)
+
+    def set_fluid_all(self, kind: str) -> None:
+        self.fluid = [kind] * 4
+
+    def set_fluid_side(self, side: int, kind: str) -> None:
+        self.fluid[_side(side)] = kind
+
+    def fluid_side(self, side: int) -> str:
+        return self.fluid[_side(side)]
+
+    def set_field_all(self, kind: str) -> None:
+        self.field = [kind] * 4
+
+    def set_field_side(self, side: int, kind: str) -> None:
+        self.field[_side(side)] = kind
+
+    def field_side(self, side: int) -> str:
+        return self.field[_side(side)]
+
+
+@dataclass
+class MhdBackgroundSpec:
+    """physics/mhd/mhd_background.hpp:67-84.  This build runs the zero-background
+    step only: a solver whose spec is enabled is refused."""
+    enabled: bool = False
+    profile: str = "uniform"
+    bx0: float = 0.0
+    by0: float = 0.0
+    bz0: float = 0.0
+    params: dict = field(default_factory=dict)
+    profile_scale: float = 1.0
+    curl_free: bool = False
 
 
 @dataclass
@@ -68,12 +108,18 @@ class MhdConfig:
     rho_floor: float = 1e-8
     p_floor: float = 1e-9
     cfl: float = 0.4
+    # restart/checkpoint identity of the dt policy (mhd_solver.hpp:70-76); kept,
+    # not interpreted, as by the solver itself
+    timestep_signature: str = ""
     boundary: MhdBoundarySpec = field(default_factory=MhdBoundarySpec)
+    background: MhdBackgroundSpec = field(default_factory=MhdBackgroundSpec)
 
 
 def _native_config(cfg: MhdConfig) -> _native.QmhdConfig:
     if cfg.geometry != "cartesian":
         raise ValueError("MhdSolver2D: geometry must be 'cartesian' in this build")
+    if cfg.background.enabled:
+        raise ValueError("MhdSolver2D: the field-split background is not supported in this build")
     if cfg.riemann != "hlld":
         raise ValueError("MhdSolver2D: device evolution supports only riemann='hlld'")
     if cfg.ct != "fd_ct_christlieb":
@@ -179,6 +225,17 @@ class MhdSolver2D:
             self._h, ctypes.byref(m), ctypes.byref(e)))
         return (m.value, e.value)
 
+    def has_background(self) -> bool:
+        """Always False: this build runs the zero-background step."""
+        return False
+
+    def seed_background(self, component: str, values) -> None:
+        # mhd_solver.cpp:543-549: a solver without an enabled background
+        # refuses B0 (std::logic_error, RuntimeError in Python)
+        raise RuntimeError(
+            "MhdSolver2D::seed_background: the field-split background is not enabled "
+            "(set background.enabled in the deck before seeding B0)")
+
     def last_positivity_substeps(self) -> int:
         return int(_native.lib().qmhd_solver_last_positivity_substeps(self._h))
 
@@ -248,3 +305,57 @@ class MhdBatch2D:
     def set_tuning(self, ctas_per_sm) -> None:
         c = (ctypes.c_int * self.PHASES)(*[int(x) for x in ctas_per_sm])
         _native.check(_native.lib().qmhd_batch_set_tuning(self._h, c))
+
+
+# -- Registry introspection (bind_mhd.cpp:101-253) ---------------------------
+# The names this build accepts, sorted like the binding's lists; the deck
+# validators select against them.  The reference's "axis" boundary, its
+# background profiles and its internal tile boundary are outside this build.
+def registered_riemann_solvers() -> List[str]:
+    return ["hlld"]
+
+
+def registered_reconstructions() -> List[str]:
+    return sorted(_ORDERS)
+
+
+def registered_integrators() -> List[str]:
+    return ["ssprk3"]
+
+
+def registered_ct_schemes() -> List[str]:
+    return ["fd_ct_christlieb"]
+
+
+def registered_positivity_limiters() -> List[str]:
+    return ["troubled_cell"]
+
+
+def registered_mhd_fluid_boundaries() -> List[str]:
+    return sorted(_BC)
+
+
+def registered_mhd_field_boundaries() -> List[str]:
+    return sorted(_BC)
+
+
+def registered_mhd_background_profiles() -> List[str]:
+    return []
+
+
+def registered_initial_conditions() -> List[str]:
+    """Built-in initial-condition generators, in the reference's kind order."""
+    return ["brio_wu", "alfven_wave", "orszag_tang", "blast", "rotor", "confined_blob"]
+
+
+def reconstruction_halo(name: str) -> int:
+    """Ghost-cell halo of the named reconstruction (bind_mhd.cpp:133-147)."""
+    if name not in _ORDERS:
+        raise ValueError(f"unknown MHD reconstruction scheme '{name}'")
+    order = _ORDERS[name]
+    return 4 if order == 7 else 3 if order == 5 else 2
+
+
+def reconstruction_order(name: str) -> int:
+    """Formal order from the halo (flux_reconstruction.hpp:65-71)."""
+    return {3: 5, 4: 7}.get(reconstruction_halo(name), 2)

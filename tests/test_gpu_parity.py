@@ -273,3 +273,13 @@ def test_ragged_grids_match_reference(ref, order, nx, ny, bc):
         err = M.state_rel_l1(read(g, shape), s.read(), ng, nx, ny)
         assert err <= STEP_TOL, (k, err)
     assert g.divergence_b_max() <= 1e-12
+
+
+def test_background_queries_on_a_live_solver():
+    """has_background / seed_background of bind_mhd.cpp:624-639 on a solver
+    built without a background: False, and B0 seeding refused with the
+    reference's message (mhd_solver.cpp:543-549)."""
+    g = gpu_solver(16, 5)
+    assert g.has_background() is False
+    with pytest.raises(RuntimeError, match="field-split background is not enabled"):
+        g.seed_background("b0x", np.zeros(g.grid().storage_size()))
