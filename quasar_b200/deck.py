@@ -159,9 +159,11 @@ class MhdDeck:
             if name not in STATE_COMPONENTS:
                 raise ValueError(f"diagnostics.fields entry {name!r} must be one of "
                                  f"{list(STATE_COMPONENTS)}")
+        kinds = set(mhd.registered_mhd_fluid_boundaries()) & set(
+            mhd.registered_mhd_field_boundaries())
         for side in range(4):
             for kind in (self.boundary.fluid[side], self.boundary.field[side]):
-                if kind not in ("periodic", "outflow", "wall"):
+                if kind not in kinds:
                     raise ValueError(f"boundary kind {kind!r} is not supported by the B200 "
                                      "solver (periodic, outflow, wall)")
             if self.boundary.fluid[side] != self.boundary.field[side]:
@@ -393,7 +395,7 @@ def load(path: Union[str, Path]) -> MhdDeck:
 
 # ---- initial states (mhd_initial_conditions.hip:59-330) ------------------------
 def nghost(reconstruction: str) -> int:
-    return {"mp7": 4, "mp5": 3, "muscl_minmod": 2}[reconstruction]
+    return mhd.reconstruction_halo(reconstruction)
 
 
 def _centres(n: int, ng: int, spacing: float, origin: float) -> np.ndarray:
