@@ -177,6 +177,42 @@ int qmhd_launch_collocate_face_to_cell(const qmhd_grid* grid, int axis, const do
 int qmhd_launch_conserved_cell_sums(const qmhd_grid* grid, const qmhd_field* u, int cylindrical,
                                     void* stream, double* mass, double* energy);
 
+/* MhdInitialConditionSpec (physics/mhd/initial_conditions.hpp:74-131), the
+ * Cartesian fields: kind 0 brio_wu, 1 alfven_wave, 2 orszag_tang, 3 blast,
+ * 4 rotor, 5 confined_blob; lx, ly, origin_x, origin_y of the spec's grid
+ * (its extents, ghost width and spacings are the qmhd_grid); left/right in
+ * the order rho, p, vx, vy, vz, bx, by, bz. */
+typedef struct qmhd_ic_spec {
+  int kind;
+  double lx, ly, origin_x, origin_y;
+  double gamma;
+  double magnetic_scale;
+  double interface_x;
+  double left[8], right[8];
+  double rho, pressure, b0, total_b0, amplitude;
+  long long wavenumber;
+  double magnetic_velocity_scale;
+  double b_uniform[3];
+  double center[2];
+  double r_in, r0, r1, rho_in, rho_out, p_in, p_out, p_core, p_ambient, rho_ambient, u0,
+      blob_half;
+} qmhd_ic_spec;
+
+/* launch_mhd_seed_initial_state (kernels.hpp:656-660): the padded initial
+ * state of `spec` into `out` (cells and faces, ghosts included), in two
+ * passes like the reference's kernels: the conserved state with the raw
+ * magnetic half-norm in the energy (also written to raw_magnetic), then the
+ * energy re-formed with the face-to-cell collocated field.  Seed errors are
+ * or-ed into the device int *status with the reference's bits
+ * (kMhdSeed*, kernels.hpp:650-655); the caller zeroes it and reads it back.
+ * cell_bx, cell_by: caller scratch as in qmhd_launch_reconstruct (they end
+ * holding the collocated field).  Cartesian only; sin, cos and hypot are
+ * CUDA's, so the sine-based and radial states may differ from the
+ * reference's CPU build in the last bits. */
+int qmhd_launch_seed_initial_state(const qmhd_grid* grid, const qmhd_ic_spec* spec,
+                                   const qmhd_field* out, double* raw_magnetic, double* cell_bx,
+                                   double* cell_by, int* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,10 +6,11 @@
 // its Cartesian, zero-background step on the B200 kernels.
 //
 // Every declaration of kernels.hpp is defined here so the solver links
-// unchanged.  The step's entry points forward to one qmhd_launch_* call each;
-// the ones outside that path (cylindrical sources, the field-split background,
-// halo packing for tiled runs, device seeding, background construction) throw
-// std::invalid_argument, as this backend's C ABI does for the same requests.
+// unchanged.  The step's entry points and the Cartesian initial-state seed
+// forward to one qmhd_launch_* call each; the ones outside that path
+// (cylindrical sources, the field-split background, halo packing for tiled
+// runs, background construction) throw std::invalid_argument, as this
+// backend's C ABI does for the same requests.
 // launch_mhd_split_energy_residual returns without work when the background is
 // inactive, as the HIP definition does (mhd_split_energy.hip:252).
 //
@@ -258,6 +259,53 @@ void launch_mhd_collocate_face_to_cell(Grid2D grid, int axis,
                                            stream));
 }
 
+void launch_mhd_seed_initial_state(const MhdInitialConditionSpec& spec, MhdField2D<Real>& out,
+                                   backend::DeviceBuffer<Real>& raw_magnetic, RadialTablesView rt,
+                                   int* status, stream_t stream) {
+  if (spec.cylindrical != 0 || rt.active)
+    outside("launch_mhd_seed_initial_state (cylindrical geometry)");
+  const qmhd_grid g = grid_of(spec.grid);
+  qmhd_ic_spec s{};
+  s.kind = static_cast<int>(spec.kind);
+  s.lx = spec.grid.lx;
+  s.ly = spec.grid.ly;
+  s.origin_x = spec.grid.origin_x;
+  s.origin_y = spec.grid.origin_y;
+  s.gamma = spec.gamma;
+  s.magnetic_scale = spec.magnetic_scale;
+  s.interface_x = spec.interface;
+  for (int c = 0; c < 8; ++c) {
+    s.left[c] = spec.left[c];
+    s.right[c] = spec.right[c];
+  }
+  s.rho = spec.rho;
+  s.pressure = spec.pressure;
+  s.b0 = spec.b0;
+  s.total_b0 = spec.total_b0;
+  s.amplitude = spec.amplitude;
+  s.wavenumber = static_cast<long long>(spec.wavenumber);
+  s.magnetic_velocity_scale = spec.magnetic_velocity_scale;
+  for (int c = 0; c < 3; ++c) s.b_uniform[c] = spec.b_uniform[c];
+  s.center[0] = spec.center[0];
+  s.center[1] = spec.center[1];
+  s.r_in = spec.r_in;
+  s.r0 = spec.r0;
+  s.r1 = spec.r1;
+  s.rho_in = spec.rho_in;
+  s.rho_out = spec.rho_out;
+  s.p_in = spec.p_in;
+  s.p_out = spec.p_out;
+  s.p_core = spec.p_core;
+  s.p_ambient = spec.p_ambient;
+  s.rho_ambient = spec.rho_ambient;
+  s.u0 = spec.u0;
+  s.blob_half = spec.blob_half;
+  const qmhd_field f = field_of(out);
+  const std::size_t n = spec.grid.storage_size();
+  check(qmhd_launch_seed_initial_state(&g, &s, &f, raw_magnetic.device_ptr(), colloc(0, n),
+                                       colloc(1, n), status, stream));
+}
+
 // ---- outside the Cartesian zero-background step --------------------------
 
 void launch_mhd_device_halo_pack(Grid2D, MhdDeviceHaloDirection,
@@ -312,11 +360,6 @@ MhdBackgroundCurlFreeResult launch_mhd_validate_background_curl_free(
 }
 void launch_mhd_fill_ghosts_background(MhdBackgroundField<Real>&, int, int, stream_t) {
   outside("launch_mhd_fill_ghosts_background");
-}
-void launch_mhd_seed_initial_state(const MhdInitialConditionSpec&, MhdField2D<Real>&,
-                                   backend::DeviceBuffer<Real>&, RadialTablesView, int*,
-                                   stream_t) {
-  outside("launch_mhd_seed_initial_state");
 }
 void launch_mhd_sample_background_profile(Grid2D, const MhdBackgroundAffineProfile&, Real, int,
                                           MhdBackgroundField<Real>&, int*, stream_t) {

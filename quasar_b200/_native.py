@@ -42,7 +42,8 @@ LAUNCH_EXPORTS = ("qmhd_launch_reconstruct", "qmhd_launch_hlld_flux", "qmhd_laun
                   "qmhd_launch_admissible_fraction", "qmhd_launch_cfl_max_rate",
                   "qmhd_launch_ct_divb_linf", "qmhd_launch_ct_divb_relative_linf",
                   "qmhd_launch_fill_ghosts_fluid", "qmhd_launch_fill_ghosts_field",
-                  "qmhd_launch_collocate_face_to_cell", "qmhd_launch_conserved_cell_sums")
+                  "qmhd_launch_collocate_face_to_cell", "qmhd_launch_conserved_cell_sums",
+                  "qmhd_launch_seed_initial_state")
 LAUNCH_SCRATCH_BYTES = 64
 
 

@@ -436,6 +436,45 @@ int qmhd_launch_collocate_face_to_cell(const qmhd_grid* grid, int axis, const do
   });
 }
 
+int qmhd_launch_seed_initial_state(const qmhd_grid* grid, const qmhd_ic_spec* spec,
+                                   const qmhd_field* out, double* raw_magnetic, double* cell_bx,
+                                   double* cell_by, int* status, void* stream) {
+  return qb::capi_guarded([&] {
+    const char* fn = "qmhd_launch_seed_initial_state";
+    const Grid g = make_grid(fn, grid, nullptr);
+    if (!spec) bad(fn, "null spec");
+    if (spec->kind < 0 || spec->kind > 5) bad(fn, "kind must be 0..5");
+    check_gamma(fn, spec->gamma);
+    if (!(std::isfinite(spec->magnetic_scale) && spec->magnetic_scale > 0.0))
+      bad(fn, "magnetic unit scale must be finite and positive");
+    if (!(std::isfinite(spec->lx) && spec->lx > 0.0 && std::isfinite(spec->ly) && spec->ly > 0.0))
+      bad(fn, "lx and ly must be finite and positive");
+    if (!raw_magnetic || !cell_bx || !cell_by || !status) bad(fn, "null scratch or status");
+    const StateP st = state_of(fn, out, cell_bx, cell_by);
+    qb::SeedSpec s{};
+    s.kind = spec->kind;
+    s.lx = spec->lx; s.ly = spec->ly; s.ox = spec->origin_x; s.oy = spec->origin_y;
+    s.gamma = spec->gamma;
+    s.magnetic_scale = spec->magnetic_scale;
+    s.interface_x = spec->interface_x;
+    for (int c = 0; c < 8; ++c) {
+      s.left[c] = spec->left[c];
+      s.right[c] = spec->right[c];
+    }
+    s.rho = spec->rho; s.pressure = spec->pressure; s.b0 = spec->b0;
+    s.total_b0 = spec->total_b0; s.amplitude = spec->amplitude;
+    s.wavenumber = spec->wavenumber; s.mvs = spec->magnetic_velocity_scale;
+    for (int c = 0; c < 3; ++c) s.b_uniform[c] = spec->b_uniform[c];
+    s.center[0] = spec->center[0]; s.center[1] = spec->center[1];
+    s.r_in = spec->r_in; s.r0 = spec->r0; s.r1 = spec->r1;
+    s.rho_in = spec->rho_in; s.rho_out = spec->rho_out; s.p_in = spec->p_in;
+    s.p_out = spec->p_out; s.p_core = spec->p_core; s.p_ambient = spec->p_ambient;
+    s.rho_ambient = spec->rho_ambient; s.u0 = spec->u0; s.blob_half = spec->blob_half;
+    qb::launch_abi_seed(g, s, st, raw_magnetic, status, as_stream(stream));
+    check_cuda(fn, cudaGetLastError());
+  });
+}
+
 int qmhd_launch_conserved_cell_sums(const qmhd_grid* grid, const qmhd_field* u, int cylindrical,
                                     void* stream, double* mass, double* energy) {
   if (cylindrical) {

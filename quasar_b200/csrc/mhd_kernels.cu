@@ -2501,6 +2501,183 @@ __global__ void k_abi_collocate(Grid g, int axis, const double* __restrict__ fac
                                             g.ny + g.ng - 1);
 }
 
+// ---- analytic initial state (mhd_initial_conditions.hip:59-340) -----------
+// Status bits of kernels.hpp:650-655.
+constexpr int kSeedDensity = 1, kSeedPressure = 2, kSeedMomentum = 4, kSeedEnergy = 8,
+              kSeedCollocation = 16, kSeedCoordinate = 32;
+
+struct SeedW {
+  double rho, p, vx, vy, vz, bx, by, bz, eoff;
+};
+
+// The generators in the reference's operation order, every product and sum
+// rounded on its own (no contraction); sin, cos and hypot are CUDA's.
+__device__ SeedW seed_eval(const SeedSpec& s, int nx, double xc, double yc) {
+  constexpr double kPi = 3.141592653589793;  // nearest double to pi
+  const double two_pi = 2.0 * kPi;
+  SeedW w{};
+  switch (s.kind) {
+    case 0: {  // brio_wu: left/right primitive states split at x = interface
+      const double* side = xc < s.interface_x ? s.left : s.right;
+      w.rho = side[0]; w.p = side[1]; w.vx = side[2]; w.vy = side[3]; w.vz = side[4];
+      w.bx = side[5]; w.by = side[6]; w.bz = side[7];
+      break;
+    }
+    case 1: {  // alfven_wave along x with the sinc cell-average factor
+      const double n = double(s.wavenumber);
+      const double k = __ddiv_rn(__dmul_rn(two_pi, n), s.lx);
+      const double phase = __dmul_rn(k, __dsub_rn(xc, s.ox));
+      const double q = __ddiv_rn(n, double(nx));
+      double fv = 1.0;
+      if (q != 0.0) {
+        const double pq = __dmul_rn(kPi, q);
+        fv = __ddiv_rn(sin(pq), pq);
+      }
+      const double inv = __ddiv_rn(copysign(s.mvs, s.total_b0), __dsqrt_rn(s.rho));
+      const double sp = sin(phase), cp = cos(phase);
+      const double a = __dmul_rn(__dmul_rn(-s.amplitude, inv), fv);
+      w.rho = s.rho; w.p = s.pressure; w.vx = 0.0;
+      w.vy = __dmul_rn(a, sp);
+      w.vz = __dmul_rn(a, cp);
+      w.bx = s.b0;
+      w.by = __dmul_rn(__dmul_rn(s.amplitude, fv), sp);
+      w.bz = __dmul_rn(__dmul_rn(s.amplitude, fv), cp);
+      const double sa = __dmul_rn(s.amplitude, s.mvs);
+      w.eoff = __dmul_rn(__dmul_rn(sa, sa), __dsub_rn(1.0, __dmul_rn(fv, fv)));
+      break;
+    }
+    case 2: {  // orszag_tang
+      const double xi = __ddiv_rn(__dsub_rn(xc, s.ox), s.lx);
+      const double eta = __ddiv_rn(__dsub_rn(yc, s.oy), s.ly);
+      const double b0 = s.b_uniform[0];
+      const double se = sin(__dmul_rn(two_pi, eta));
+      w.rho = __dmul_rn(s.gamma, s.gamma); w.p = s.gamma;
+      w.vx = -se;
+      w.vy = sin(__dmul_rn(two_pi, xi));
+      w.bx = __dmul_rn(-b0, se);
+      w.by = __dmul_rn(b0, sin(__dmul_rn(2.0 * two_pi, xi)));
+      break;
+    }
+    case 3: {  // blast: pressure disk
+      const double r = hypot(__dsub_rn(xc, s.center[0]), __dsub_rn(yc, s.center[1]));
+      w.rho = s.rho_ambient;
+      w.p = r < s.r_in ? s.p_core : s.p_ambient;
+      w.bx = s.b_uniform[0]; w.by = s.b_uniform[1]; w.bz = s.b_uniform[2];
+      break;
+    }
+    case 4: {  // rotor: rigid disk with a linear taper
+      const double rx = __dsub_rn(xc, s.center[0]), ry = __dsub_rn(yc, s.center[1]);
+      const double r = hypot(rx, ry);
+      double f = __ddiv_rn(__dsub_rn(s.r1, r), __dsub_rn(s.r1, s.r0));
+      f = fmin(fmax(f, 0.0), 1.0);
+      const bool inside = r <= s.r0;
+      if (inside) f = 1.0;
+      if (r >= s.r1) f = 0.0;
+      double speed = 0.0;
+      if (inside) speed = __ddiv_rn(s.u0, s.r0);
+      else if (r < s.r1) speed = __ddiv_rn(__dmul_rn(f, s.u0), r);
+      w.rho = __dadd_rn(s.rho_out, __dmul_rn(f, __dsub_rn(s.rho_in, s.rho_out)));
+      w.p = s.p_ambient;
+      w.vx = __dmul_rn(-speed, ry);
+      w.vy = __dmul_rn(speed, rx);
+      w.bx = s.b_uniform[0]; w.by = s.b_uniform[1]; w.bz = s.b_uniform[2];
+      break;
+    }
+    default: {  // confined_blob: dense square, uniform bz
+      const bool inside = fabs(__dsub_rn(xc, s.center[0])) <= s.blob_half &&
+                          fabs(__dsub_rn(yc, s.center[1])) <= s.blob_half;
+      w.rho = inside ? s.rho_in : s.rho_out;
+      w.p = inside ? s.p_in : s.p_out;
+      w.bz = s.b_uniform[2];
+      break;
+    }
+  }
+  return w;
+}
+
+// Pass 1 (mhd_initial_conditions.hip:211-282): one padded cell per thread;
+// the faces of a cell take its centre value.
+__global__ void __launch_bounds__(256) k_seed_pass1(Grid g, SeedSpec s, StateP u, double* raw,
+                                                    int* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - g.ng;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - g.ng;
+  if (i >= g.nx + g.ng || j >= g.ny + g.ng) return;
+  const double xc = fma(double(i) + 0.5, g.dx, s.ox);
+  const double yc = fma(double(j) + 0.5, g.dy, s.oy);
+  if (!(isfinite(xc) && isfinite(yc))) {
+    atomicOr(status, kSeedCoordinate);
+    return;
+  }
+  const SeedW w = seed_eval(s, g.nx, xc, yc);
+  if (!(isfinite(w.rho) && w.rho > 0.0)) {
+    atomicOr(status, kSeedDensity);
+    return;
+  }
+  if (!(isfinite(w.p) && w.p > 0.0)) {
+    atomicOr(status, kSeedPressure);
+    return;
+  }
+  const double kinetic = kin_vel(w.rho, w.vx, w.vy, w.vz);
+  const double magnetic = half_sq3(w.bx, w.by, w.bz);
+  const double energy = __dadd_rn(
+      __dadd_rn(__dadd_rn(__ddiv_rn(w.p, __dsub_rn(s.gamma, 1.0)), kinetic), magnetic), w.eoff);
+  const double mx = __dmul_rn(w.rho, w.vx), my = __dmul_rn(w.rho, w.vy),
+               mz = __dmul_rn(w.rho, w.vz);
+  if (!(isfinite(mx) && isfinite(my) && isfinite(mz))) {
+    atomicOr(status, kSeedMomentum);
+    return;
+  }
+  if (!isfinite(energy)) {
+    atomicOr(status, kSeedEnergy);
+    return;
+  }
+  const long long k = g.idx(i, j);
+  u.c[0][k] = w.rho;
+  u.c[1][k] = mx;
+  u.c[2][k] = my;
+  u.c[3][k] = mz;
+  u.c[4][k] = energy;
+  u.c[5][k] = __dmul_rn(s.magnetic_scale, w.bx);
+  u.c[6][k] = __dmul_rn(s.magnetic_scale, w.by);
+  u.c[7][k] = __dmul_rn(s.magnetic_scale, w.bz);
+  raw[k] = magnetic;
+}
+
+// Pass 2 (mhd_initial_conditions.hip:284-340): E = (E - raw) + |B_c|^2 / 2
+// with B_c the collocated field the solver's EOS reads, then the preflight
+// on the conserved arrays.
+__global__ void __launch_bounds__(256) k_seed_recollocate(Grid g, double gamma, StateP u,
+                                                          const double* raw, int* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - g.ng;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - g.ng;
+  if (i >= g.nx + g.ng || j >= g.ny + g.ng) return;
+  const long long k = g.idx(i, j);
+  const double bxc = u.bxc[k], byc = u.byc[k];
+  if (!(isfinite(bxc) && isfinite(byc))) {
+    atomicOr(status, kSeedCollocation);
+    return;
+  }
+  const double adjusted =
+      __dadd_rn(__dsub_rn(u.c[4][k], raw[k]), half_sq3(bxc, byc, u.c[7][k]));
+  if (!isfinite(adjusted)) {
+    atomicOr(status, kSeedEnergy);
+    return;
+  }
+  u.c[4][k] = adjusted;
+  const double rho = u.c[0][k];
+  if (!(isfinite(rho) && rho > 0.0)) {
+    atomicOr(status, kSeedDensity);
+    return;
+  }
+  const St st{rho, u.c[1][k], u.c[2][k], u.c[3][k], adjusted, bxc, byc, u.c[7][k]};
+  const double p = pressure(st, gamma);
+  if (!isfinite(p)) {
+    atomicOr(status, kSeedEnergy);
+    return;
+  }
+  if (!(p > 0.0)) atomicOr(status, kSeedPressure);
+}
+
 // One side's ghost layers, fluid (parts 1) or field (parts 2)
 // (mhd_boundary_hip.hip:66-218).
 __global__ void k_abi_fill_side(Grid g, StateP u, int side, int mode, int parts) {
@@ -2683,6 +2860,15 @@ void launch_abi_collocate(const Grid& g, int axis, const double* face, double* c
   if (g.ng == 2) k_abi_collocate<4><<<grid, block, 0, s>>>(g, axis, face, cell);
   else if (g.ng == 3) k_abi_collocate<6><<<grid, block, 0, s>>>(g, axis, face, cell);
   else k_abi_collocate<8><<<grid, block, 0, s>>>(g, axis, face, cell);
+}
+
+void launch_abi_seed(const Grid& g, const SeedSpec& spec, const StateP& out, double* raw,
+                     int* status, cudaStream_t s) {
+  const dim3 block(kBX, 8), grid(cdiv(g.nx + 2 * g.ng, kBX), cdiv(g.ny + 2 * g.ng, 8));
+  k_seed_pass1<<<grid, block, 0, s>>>(g, spec, out, raw, status);
+  launch_abi_collocate(g, 0, out.c[5], out.bxc, s);
+  launch_abi_collocate(g, 1, out.c[6], out.byc, s);
+  k_seed_recollocate<<<grid, block, 0, s>>>(g, spec.gamma, out, raw, status);
 }
 
 void launch_abi_fill_side(const Grid& g, const StateP& u, int side, int mode, int parts,

@@ -138,6 +138,28 @@ void launch_abi_cfl_rate(const Grid& g, const IfaceP& ix, const IfaceP& iy, int 
                          double gamma, unsigned long long* max_rate, cudaStream_t s);
 void launch_abi_set_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s);
 
+// Analytic initial state of the reference's Cartesian generators
+// (MhdInitialConditionSpec, physics/mhd/initial_conditions.hpp:74-131):
+// kind 0 brio_wu, 1 alfven_wave, 2 orszag_tang, 3 blast, 4 rotor,
+// 5 confined_blob.
+struct SeedSpec {
+  int kind;
+  double lx, ly, ox, oy, gamma, magnetic_scale;
+  double interface_x, left[8], right[8];
+  double rho, pressure, b0, total_b0, amplitude;
+  long long wavenumber;
+  double mvs, b_uniform[3], center[2];
+  double r_in, r0, r1, rho_in, rho_out, p_in, p_out, p_core, p_ambient, rho_ambient, u0,
+      blob_half;
+};
+// Both passes of launch_mhd_seed_initial_state over the padded grid: the
+// conserved state with the raw magnetic half-norm in the energy (out.c,
+// raw), the face-to-cell collocation of the seeded faces (out.bxc, out.byc),
+// and the energy re-formed from the collocated field.  Seed errors are
+// or-ed into *status with the reference's bit values.
+void launch_abi_seed(const Grid& g, const SeedSpec& spec, const StateP& out, double* raw,
+                     int* status, cudaStream_t s);
+
 // ---- batched step: many independent instances per launch -----------------
 // One record per instance and stage: the instance's stage arguments (a.u is
 // the stage input), its live register (update and admissibility base) and the

@@ -43,6 +43,20 @@ class CflRate(ctypes.Structure):
     _fields_ = [("scaled_max_rate", _d), ("rate_scale", _d)]
 
 
+class IcSpec(ctypes.Structure):
+    """MhdInitialConditionSpec, Cartesian fields (kind 0 brio_wu, 1 alfven_wave,
+    2 orszag_tang, 3 blast, 4 rotor, 5 confined_blob)."""
+    _fields_ = [("kind", _i), ("lx", _d), ("ly", _d), ("origin_x", _d), ("origin_y", _d),
+                ("gamma", _d), ("magnetic_scale", _d), ("interface_x", _d),
+                ("left", _d * 8), ("right", _d * 8),
+                ("rho", _d), ("pressure", _d), ("b0", _d), ("total_b0", _d), ("amplitude", _d),
+                ("wavenumber", ctypes.c_longlong), ("magnetic_velocity_scale", _d),
+                ("b_uniform", _d * 3), ("center", _d * 2),
+                ("r_in", _d), ("r0", _d), ("r1", _d), ("rho_in", _d), ("rho_out", _d),
+                ("p_in", _d), ("p_out", _d), ("p_core", _d), ("p_ambient", _d),
+                ("rho_ambient", _d), ("u0", _d), ("blob_half", _d)]
+
+
 _P = ctypes.POINTER
 _flags = _P(_i)
 
@@ -65,6 +79,7 @@ def declare(L) -> None:
     L.qmhd_launch_fill_ghosts_field.argtypes = [g, f, _i, _i, _vp]
     L.qmhd_launch_collocate_face_to_cell.argtypes = [g, _i, _vp, _vp, _vp]
     L.qmhd_launch_conserved_cell_sums.argtypes = [g, f, _i, _vp, _P(_d), _P(_d)]
+    L.qmhd_launch_seed_initial_state.argtypes = [g, _P(IcSpec), f, _vp, _vp, _vp, _vp, _vp]
 
 
 def _ptr(t) -> int | None:
@@ -191,3 +206,12 @@ def conserved_cell_sums(grid, u, stream=None) -> tuple[float, float]:
     _native.check(_native.lib().qmhd_launch_conserved_cell_sums(
         ctypes.byref(grid), ctypes.byref(u), 0, _stream(stream), ctypes.byref(m), ctypes.byref(e)))
     return m.value, e.value
+
+
+def seed_initial_state(grid, spec, out, raw_magnetic, cell_bx, cell_by, status,
+                       stream=None) -> None:
+    """launch_mhd_seed_initial_state; status: a device int32 tensor the
+    caller zeroes and reads back (the reference's kMhdSeed* bits)."""
+    _native.check(_native.lib().qmhd_launch_seed_initial_state(
+        ctypes.byref(grid), ctypes.byref(spec), ctypes.byref(out), _ptr(raw_magnetic),
+        _ptr(cell_bx), _ptr(cell_by), _ptr(status), _stream(stream)))

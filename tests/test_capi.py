@@ -46,7 +46,7 @@ def test_launch_interface_names_every_reference_seam_entry():
     want = ("reconstruct", "hlld_flux", "flux_difference", "ct_emf_prepare", "ct_emf_finish",
             "emf_curl_rate", "rk_stage", "admissible_fraction", "cfl_max_rate", "ct_divb_linf",
             "ct_divb_relative_linf", "fill_ghosts_fluid", "fill_ghosts_field",
-            "collocate_face_to_cell", "conserved_cell_sums")
+            "collocate_face_to_cell", "conserved_cell_sums", "seed_initial_state")
     assert set("qmhd_launch_" + w for w in want) == set(declared_symbols("quasar_mhd_launch.h"))
 
 
