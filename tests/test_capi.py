@@ -93,6 +93,21 @@ def test_launch_interface_rejects_bad_arguments_before_any_launch():
     with pytest.raises(ValueError, match="collocation scratch"):
         _native.check(lib.qmhd_launch_reconstruct(ctypes.byref(g), ctypes.byref(u), None, None, 0,
                                                   ctypes.byref(iface), 7, per, 5 / 3, None, 1))
+    spec = L.IcSpec()
+    spec.kind, spec.gamma, spec.magnetic_scale, spec.lx, spec.ly = 9, 5 / 3, 1.0, 1.0, 1.0
+    seed = lambda: _native.check(lib.qmhd_launch_seed_initial_state(  # noqa: E731
+        ctypes.byref(g), ctypes.byref(spec), ctypes.byref(u), None, None, None, None, None))
+    with pytest.raises(ValueError, match="kind"):
+        seed()
+    spec.kind, spec.gamma = 2, 1.0
+    with pytest.raises(ValueError, match="gamma"):
+        seed()
+    spec.gamma, spec.magnetic_scale = 5 / 3, 0.0
+    with pytest.raises(ValueError, match="magnetic unit scale"):
+        seed()
+    spec.magnetic_scale = 1.0
+    with pytest.raises(ValueError, match="null scratch or status"):
+        seed()
     with pytest.raises(ValueError, match="ownership"):
         _native.check(lib.qmhd_launch_hlld_flux(ctypes.byref(g), ctypes.byref(iface), 0,
                                                 ctypes.byref(u), per, 5 / 3, None, 0, 7,
