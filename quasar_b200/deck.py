@@ -45,6 +45,8 @@ _PRIMITIVE_KEYS = ("rho", "p", "vx", "vy", "vz", "bx", "by", "bz")
 _TOP_LEVEL_KEYS = {"units", "domain", "geometry", "numerics", "initial", "time",
                    "diagnostics", "boundary", "background_field"}
 INITIAL_TYPES = ("brio_wu", "alfven_wave", "orszag_tang", "blast", "rotor", "confined_blob")
+MAX_GRID_DIM = 1 << 16  # cells per axis (io.py:83-84)
+MAX_GRID_CELLS = 1 << 30
 _KIND = {name: k for k, name in enumerate(INITIAL_TYPES)}
 MU0 = 4.0e-7 * math.pi
 SQRT_MU0 = math.sqrt(MU0)
@@ -125,8 +127,13 @@ class MhdDeck:
         if self.geometry != "cartesian":
             raise ValueError("geometry 'cylindrical' is not supported by the B200 solver")
         d = self.domain
-        if _exact_int(d.nx, "domain.nx") <= 0 or _exact_int(d.ny, "domain.ny") <= 0:
+        nx, ny = _exact_int(d.nx, "domain.nx"), _exact_int(d.ny, "domain.ny")
+        if nx <= 0 or ny <= 0:
             raise ValueError("domain.nx and domain.ny must be positive")
+        if nx > MAX_GRID_DIM or ny > MAX_GRID_DIM:
+            raise ValueError(f"domain.nx/ny must be <= {MAX_GRID_DIM} (got {nx}x{ny})")
+        if nx * ny > MAX_GRID_CELLS:
+            raise ValueError(f"domain.nx*ny must be <= {MAX_GRID_CELLS} cells")
         for name in ("lx_m", "ly_m"):
             v = getattr(d, name)
             if not (math.isfinite(v) and v > 0.0):
@@ -134,9 +141,31 @@ class MhdDeck:
         for name in ("origin_x_m", "origin_y_m"):
             if not math.isfinite(getattr(d, name)):
                 raise ValueError(f"domain.{name} must be finite")
+        # io.py:434-449: the grid must stay representable in binary64 (upper
+        # bounds, spacings, and distinct first and last cell centres)
+        x0, y0 = float(d.origin_x_m), float(d.origin_y_m)
+        x1, y1 = x0 + float(d.lx_m), y0 + float(d.ly_m)
+        for v, what in ((x1, "domain upper x bound"), (y1, "domain upper y bound")):
+            if not math.isfinite(v):
+                raise ValueError(f"{what} must be finite")
+        dx, dy = float(d.lx_m) / nx, float(d.ly_m) / ny
+        for v, what in ((dx, "domain x spacing"), (dy, "domain y spacing")):
+            if not (math.isfinite(v) and v > 0.0):
+                raise ValueError(f"{what} must be finite and positive")
+        if (x0 + 0.5 * dx == x0 or x0 + (nx - 0.5) * dx == x1
+                or y0 + 0.5 * dy == y0 or y0 + (ny - 0.5) * dy == y1):
+            raise ValueError("domain cell coordinates collapse in floating-point precision")
         n = self.numerics
         if not (math.isfinite(n.gamma) and n.gamma > 1.0):
             raise ValueError("numerics.gamma must be finite and greater than one")
+        for value, names, context in (
+                (n.reconstruction, mhd.registered_reconstructions(), "numerics.reconstruction"),
+                (n.riemann, mhd.registered_riemann_solvers(), "numerics.riemann"),
+                (n.integrator, mhd.registered_integrators(), "numerics.integrator"),
+                (n.ct, mhd.registered_ct_schemes(), "numerics.ct"),
+                (n.positivity, mhd.registered_positivity_limiters(), "numerics.positivity")):
+            if value not in names:
+                raise ValueError(f"{context} {value!r} must be one of {sorted(names)}")
         if not (math.isfinite(n.cfl) and n.cfl > 0.0):
             raise ValueError("numerics.cfl must be finite and positive")
         if self.initial is None:
@@ -153,7 +182,10 @@ class MhdDeck:
             raise ValueError("time.steps must be positive")
         if t.t_end is not None and not (math.isfinite(t.t_end) and t.t_end > 0.0):
             raise ValueError("time.t_end must be positive and finite")
-        if self.diagnostics.cadence < 0:
+        if (not isinstance(self.diagnostics.output_path, str)
+                or not self.diagnostics.output_path.strip()):
+            raise ValueError("diagnostics.output_path must be a non-empty string")
+        if _exact_int(self.diagnostics.cadence, "diagnostics.cadence") < 0:
             raise ValueError("diagnostics.cadence must be non-negative")
         for name in self.diagnostics.fields:
             if name not in STATE_COMPONENTS:
@@ -161,22 +193,36 @@ class MhdDeck:
                                  f"{list(STATE_COMPONENTS)}")
         kinds = set(mhd.registered_mhd_fluid_boundaries()) & set(
             mhd.registered_mhd_field_boundaries())
+        fl, fd = self.boundary.fluid, self.boundary.field
         for side in range(4):
-            for kind in (self.boundary.fluid[side], self.boundary.field[side]):
+            for part, kind in (("fluid", fl[side]), ("field", fd[side])):
+                if kind == "internal":
+                    raise ValueError(f"boundary.{part}[{side}] = 'internal' is reserved for "
+                                     "the distributed tile runtime")
                 if kind not in kinds:
                     raise ValueError(f"boundary kind {kind!r} is not supported by the B200 "
                                      "solver (periodic, outflow, wall)")
+        # io.py:550-564
+        for side in range(4):
+            if (fl[side] == "periodic") != (fd[side] == "periodic"):
+                raise ValueError("fluid and field periodicity must match on every side")
+        for lo in (0, 2):
+            if ((fl[lo] == "periodic") != (fl[lo + 1] == "periodic")
+                    or (fd[lo] == "periodic") != (fd[lo + 1] == "periodic")):
+                raise ValueError("periodic boundaries must be selected on both sides of an axis")
+        for side in range(4):
             if self.boundary.fluid[side] != self.boundary.field[side]:
                 raise ValueError("fluid and field boundaries must match per side in the B200 "
                                  "solver")
 
 
 def _exact_int(value, context: str) -> int:
-    if isinstance(value, bool):
-        raise ValueError(f"{context} must be an integer")
+    """An integer as YAML gives it (io.py:100-115): booleans and floats,
+    integral-looking ones such as 16.0 included, are refused so a misspelt
+    deck cannot silently change its grid, run length, cadence or mode."""
+    if isinstance(value, (bool, np.bool_)):
+        raise ValueError(f"{context} must be an integer, not a boolean")
     if isinstance(value, (int, np.integer)):
-        return int(value)
-    if isinstance(value, float) and value.is_integer():
         return int(value)
     raise ValueError(f"{context} must be an integer")
 
@@ -371,6 +417,10 @@ def parse(data: dict) -> MhdDeck:
     boundary = BoundaryConfig(fluid=_side_map(b.get("fluid"), "boundary.fluid"),
                               field=_side_map(b.get("field"), "boundary.field"))
     bg = _mapping(data.get("background_field"), "background_field")
+    _reject_unknown(bg, {"enabled", "profile", "bx0", "by0", "bz0", "params", "file", "a_file",
+                         "conductors"}, "background_field")
+    if not isinstance(bg.get("enabled", False), (bool, np.bool_)):
+        raise ValueError("background_field.enabled must be a boolean")
     if bg.get("enabled", False):
         raise ValueError("background_field is not supported by the B200 solver "
                          "(field-split B0 is out of its scope)")
@@ -382,10 +432,35 @@ def parse(data: dict) -> MhdDeck:
     return deck
 
 
-def load(path: Union[str, Path]) -> MhdDeck:
+def _yaml_load(text: str):
+    """One YAML document with duplicate mapping keys refused (a later key
+    would otherwise silently replace the earlier one)."""
     import yaml
+
+    class Loader(yaml.SafeLoader):
+        pass
+
+    def mapping(loader, node, deep=False):
+        seen = set()
+        for key_node, _ in node.value:
+            key = loader.construct_object(key_node, deep=deep)
+            try:
+                dup = key in seen
+            except TypeError:
+                dup = False
+            if dup:
+                raise ValueError(f"duplicate YAML key {key!r} at line "
+                                 f"{key_node.start_mark.line + 1}")
+            seen.add(key)
+        return yaml.SafeLoader.construct_mapping(loader, node, deep=deep)
+
+    Loader.add_constructor(yaml.resolver.BaseResolver.DEFAULT_MAPPING_TAG, mapping)
+    return yaml.load(text, Loader=Loader)  # noqa: S506 (a SafeLoader subclass)
+
+
+def load(path: Union[str, Path]) -> MhdDeck:
     with open(path) as fh:
-        data = yaml.safe_load(fh)
+        data = _yaml_load(fh.read())
     if not isinstance(data, dict):
         raise ValueError(f"{path}: top-level YAML must be a mapping")
     deck = parse(data)

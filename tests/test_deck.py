@@ -34,7 +34,8 @@ def test_decks_parse_and_defaults():
     (lambda r: r["numerics"].update(gamma=1.0), "gamma"),
     (lambda r: r["initial"].update(type="tearing"), "initial.type"),
     (lambda r: r["initial"]["params"].update(extra=2), "unknown key"),
-    (lambda r: r["boundary"].update(fluid="wall"), "match per side"),
+    (lambda r: r["boundary"].update(fluid="wall"), "periodicity must match"),
+    (lambda r: r["boundary"].update(fluid="wall", field="outflow"), "match per side"),
     (lambda r: r["boundary"].update(fluid="axis", field="axis"), "not supported"),
     (lambda r: r["time"].update(steps=0), "time.steps"),
     (lambda r: r["diagnostics"].update(fields=["temperature"]), "diagnostics.fields"),
