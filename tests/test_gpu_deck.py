@@ -72,3 +72,16 @@ def test_deck_run_matches_reference_solver(ref, tmp_path, name, recon):
     assert z["snapshot_steps"].tolist() == [4] and z["snapshot_state_rho"].shape == (1, dm.ny, dm.nx)
     if name == "orszag_tang":
         assert "mass_initial" in z and "energy_initial" in z
+
+
+def test_explicit_dt_above_cfl_limit_fails_before_output(tmp_path):
+    """An explicit dt far above the CFL limit passes deck validation (no
+    solver exists there) and is refused by the solver's checked step before
+    any archive is written, as in the reference's CLI."""
+    data = copy.deepcopy(D.decks(16, "mp5")["orszag_tang"])
+    data["time"]["dt_s"] = 1.0e6
+    path = tmp_path / "deck.yaml"
+    path.write_text(yaml.safe_dump(data))
+    with pytest.raises(ValueError, match="CFL"):
+        Q.run(str(path))
+    assert not (tmp_path / "out.npz").exists()
