@@ -60,7 +60,7 @@ typedef struct qmhd_iface {
   double* right[8];
 } qmhd_iface;
 
-/* EmfField2D (physics/mhd/mhd_field.hpp) as this build forms it: the upwind
+/* EmfField2D (physics/mhd/mhd_field.hpp) as this library forms it: the upwind
  * face E_z of each direction with its one-dimensional "no jump" proof, the
  * cell-average E_z, and the corner E_z at the lower-left corner of each cell
  * (the reference's ez_edge). */
@@ -74,7 +74,7 @@ typedef struct qmhd_emf {
 } qmhd_emf;
 
 /* ScaledCflRate (kernels.hpp:483-486): true max rate = scaled_max_rate /
- * rate_scale.  This build always reports rate_scale 1; an aggregate that
+ * rate_scale.  This library always reports rate_scale 1; an aggregate that
  * overflows reports +inf. */
 typedef struct qmhd_cfl_rate {
   double scaled_max_rate;
@@ -171,7 +171,7 @@ int qmhd_launch_collocate_face_to_cell(const qmhd_grid* grid, int axis, const do
                                        double* cell, void* stream);
 
 /* launch_mhd_conserved_cell_sums (kernels.hpp:412-414): compensated mass and
- * energy totals of the interior cells, returned to the host (this build
+ * energy totals of the interior cells, returned to the host (this library
  * finishes the sum on the device; the scratch rule of
  * qmhd_conserved_cell_totals_device applies). */
 int qmhd_launch_conserved_cell_sums(const qmhd_grid* grid, const qmhd_field* u, int cylindrical,

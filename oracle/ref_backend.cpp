@@ -69,26 +69,26 @@ void device_synchronize(stream_t) {}
 namespace quasar::mhd {
 MhdBackgroundAffineProfile lower_affine_background_profile(
     const numerics::IMhdBackgroundProfile&, const std::string&) {
-  throw std::logic_error("background profiles are not part of this build");
+  throw std::logic_error("background profiles are not part of this library");
 }
 void build_background_from_profile(const MhdBackgroundBuildSpec&,
                                    MhdBackgroundField<Real>&,
                                    backend::stream_t) {
-  throw std::logic_error("background profiles are not part of this build");
+  throw std::logic_error("background profiles are not part of this library");
 }
 }  // namespace quasar::mhd
 
 namespace quasar::numerics {
 std::vector<RadialStencilRow> solve_radial_rows(
     const std::vector<RadialRowSpec>&, backend::stream_t) {
-  throw std::logic_error("cylindrical tables are not part of this build");
+  throw std::logic_error("cylindrical tables are not part of this library");
 }
 std::vector<RadialStencilRow> radial_gauss_weight_rows(
     const std::vector<RadialGaussSpec>&, backend::stream_t) {
-  throw std::logic_error("cylindrical tables are not part of this build");
+  throw std::logic_error("cylindrical tables are not part of this library");
 }
 std::vector<Real> radial_face_extrapolation_factors(
     const std::vector<RadialExtrapolationSpec>&, backend::stream_t) {
-  throw std::logic_error("cylindrical tables are not part of this build");
+  throw std::logic_error("cylindrical tables are not part of this library");
 }
 }  // namespace quasar::numerics

@@ -3,7 +3,7 @@
     python -m quasar_b200.deck run path/to/input.yaml [--steps-override N]
 
 Drop-in for `python -m quasar.mhd.cli run` (python/quasar/mhd/cli.py) on the
-decks this build evolves: Cartesian geometry, no static background field,
+decks this library evolves: Cartesian geometry, no static background field,
 reconstruction muscl_minmod / mp5 / mp7 with HLLD, CT, SSP-RK3 and the
 troubled-cell positivity controller, periodic / outflow / wall boundaries
 (the same per side for fluid and field).  Everything else is rejected with a

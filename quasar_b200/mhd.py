@@ -82,7 +82,7 @@ class MhdBoundarySpec:
 
 @dataclass
 class MhdBackgroundSpec:
-    """physics/mhd/mhd_background.hpp:67-84.  This build runs the zero-background
+    """physics/mhd/mhd_background.hpp:67-84.  This library runs the zero-background
     step only: a solver whose spec is enabled is refused."""
     enabled: bool = False
     profile: str = "uniform"
@@ -117,9 +117,9 @@ class MhdConfig:
 
 def _native_config(cfg: MhdConfig) -> _native.QmhdConfig:
     if cfg.geometry != "cartesian":
-        raise ValueError("MhdSolver2D: geometry must be 'cartesian' in this build")
+        raise ValueError("MhdSolver2D: geometry must be 'cartesian' in this library")
     if cfg.background.enabled:
-        raise ValueError("MhdSolver2D: the field-split background is not supported in this build")
+        raise ValueError("MhdSolver2D: the field-split background is not supported in this library")
     if cfg.riemann != "hlld":
         raise ValueError("MhdSolver2D: device evolution supports only riemann='hlld'")
     if cfg.ct != "fd_ct_christlieb":
@@ -137,14 +137,14 @@ def _native_config(cfg: MhdConfig) -> _native.QmhdConfig:
     if cfg.grid.nghost > 0 and cfg.grid.nghost != required:
         raise ValueError(
             f"MhdSolver2D: grid nghost ({cfg.grid.nghost}) must equal the reconstruction "
-            f"scheme's halo ({required}) in this build")
+            f"scheme's halo ({required}) in this library")
     bc = []
     for side in range(4):
         f, b = cfg.boundary.fluid[side], cfg.boundary.field[side]
         if f not in _BC or b not in _BC:
             raise ValueError(f"MhdSolver2D: unknown boundary '{f if f not in _BC else b}'")
         if f != b:
-            raise ValueError("MhdSolver2D: fluid and field boundaries must match per side in this build")
+            raise ValueError("MhdSolver2D: fluid and field boundaries must match per side in this library")
         bc.append(_BC[f])
     c = _native.QmhdConfig()
     c.nx, c.ny = int(cfg.grid.nx), int(cfg.grid.ny)
@@ -226,7 +226,7 @@ class MhdSolver2D:
         return (m.value, e.value)
 
     def has_background(self) -> bool:
-        """Always False: this build runs the zero-background step."""
+        """Always False: this library runs the zero-background step."""
         return False
 
     def seed_background(self, component: str, values) -> None:
@@ -308,9 +308,9 @@ class MhdBatch2D:
 
 
 # -- Registry introspection (bind_mhd.cpp:101-253) ---------------------------
-# The names this build accepts, sorted like the binding's lists; the deck
+# The names this library accepts, sorted like the binding's lists; the deck
 # validators select against them.  The reference's "axis" boundary, its
-# background profiles and its internal tile boundary are outside this build.
+# background profiles and its internal tile boundary are outside this library.
 def registered_riemann_solvers() -> List[str]:
     return ["hlld"]
 
