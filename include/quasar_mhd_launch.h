@@ -5,6 +5,10 @@
  * step (src/physics/mhd/mhd_solver.cpp:680-800).  Each entry point below
  * names the declaration it replaces (kernels.hpp:line).  quasar_mhd.h is the
  * other seam (the solver class); both drive the same sm_100a kernels.
+ * launch_mhd_split_energy_residual (kernels.hpp:320-329) has no entry here:
+ * it does nothing when the background field is off (mhd_split_energy.hip:252),
+ * the only mode this library runs, so a forwarding layer defines it as that
+ * no-op.
  *
  * Conventions, as the reference states them (kernels.hpp:18-25):
  *   - every pointer is device memory of the calling thread's current device,
