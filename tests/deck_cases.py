@@ -41,7 +41,9 @@ def decks(n=24, recon="mp5"):
 def ref_params(deck):
     """The reference's spec scalars for a parsed deck (io.py:922-995)."""
     p, t = deck.initial.params, deck.initial.type
-    out = {}
+    # SI decks give B in tesla and the solver evolves B / sqrt(mu0)
+    inv_sqrt_mu0 = 1.0 / math.sqrt(4.0e-7 * math.pi) if deck.units == "SI" else 1.0
+    out = {"magnetic_scale": inv_sqrt_mu0}
     if t == "brio_wu":
         keys = ("rho", "p", "vx", "vy", "vz", "bx", "by", "bz")
         out["interface"] = float(p.get("interface", 0.5))
@@ -52,7 +54,8 @@ def ref_params(deck):
         out.update(rho=float(p.get("rho", 1.0)), pressure=float(p.get("p", 0.1)),
                    b0=float(p.get("b0", 1.0)), total_b0=float(p.get("b0", 1.0)),
                    amplitude=float(p.get("amplitude", 1e-6)),
-                   wavenumber=float(p.get("wavenumber", 1)))
+                   wavenumber=float(p.get("wavenumber", 1)),
+                   magnetic_velocity_scale=inv_sqrt_mu0)
     elif t == "orszag_tang":
         out.update(bx=float(p.get("b0", 1.0)))
     elif t == "blast":

@@ -68,8 +68,13 @@ def test_output_path_is_confined(tmp_path):
 @pytest.mark.skipif(not M.ref_available(), reason="reference build (oracle/_ref) absent")
 @pytest.mark.parametrize("name", ["orszag_tang", "rotor", "blast", "brio_wu", "alfven_wave"])
 @pytest.mark.parametrize("recon", ["mp5", "mp7"])
-def test_first_pass_matches_reference_seed_bitwise(ref, name, recon):
-    d = Q.parse(copy.deepcopy(D.decks(recon=recon)[name]))
+@pytest.mark.parametrize("units", ["normalized", "SI"])
+def test_first_pass_matches_reference_seed_bitwise(ref, name, recon, units):
+    """SI decks carry B in tesla: the seed scales it (and, for the Alfven
+    wave, its velocity eigen-relation) by 1/sqrt(mu0)."""
+    raw = copy.deepcopy(D.decks(recon=recon)[name])
+    raw["units"] = units
+    d = Q.parse(raw)
     ng = Q.nghost(recon)
     ours, _ = Q.build_initial_state_pass1(d, ng)
     dm = d.domain
