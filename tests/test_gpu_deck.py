@@ -26,8 +26,11 @@ def _ref_state(ref, d, recon):
 
 @pytest.mark.parametrize("name", ["orszag_tang", "rotor", "blast", "brio_wu", "alfven_wave"])
 @pytest.mark.parametrize("recon", ["mp5", "mp7"])
-def test_initial_state_matches_reference_seed(ref, name, recon):
-    d = Q.parse(copy.deepcopy(D.decks(recon=recon)[name]))
+@pytest.mark.parametrize("units", ["normalized", "SI"])
+def test_initial_state_matches_reference_seed(ref, name, recon, units):
+    raw = copy.deepcopy(D.decks(recon=recon)[name])
+    raw["units"] = units
+    d = Q.parse(raw)
     ours = Q.build_initial_state(d, Q.nghost(recon))
     want = _ref_state(ref, d, recon)
     for c, comp in enumerate(Q.STATE_COMPONENTS):
