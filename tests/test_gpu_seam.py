@@ -221,9 +221,10 @@ def test_reference_seed_on_seam_matches_cpu_seed(seam, ref, name, recon):
     """The reference's own build_initial_state (initial_conditions.cpp:166-213)
     seeding through launch_mhd_seed_initial_state, here this project's
     kernels, against the same call in the reference's CPU build.  Bit for bit
-    where the generator is plain arithmetic (brio_wu); elsewhere CUDA's sin,
-    cos and hypot may differ from the C library's in the last bit, so every
-    component agrees within 8 ulp of its largest magnitude."""
+    for brio_wu and blast; where CUDA's sin, cos or hypot differ from the C
+    library's in the last bit (a few Orszag-Tang and Alfven-wave cells, two
+    rotor taper cells), every component agrees within 8 ulp of its largest
+    magnitude."""
     import copy
     import deck_cases as D
     from quasar_b200 import deck as Q
@@ -237,7 +238,7 @@ def test_reference_seed_on_seam_matches_cpu_seed(seam, ref, name, recon):
     for c, comp in enumerate(Q.STATE_COMPONENTS):
         a, b = got[c], want[c]
         assert np.all(np.isfinite(a)), (name, comp)
-        if name == "brio_wu":
+        if name in ("brio_wu", "blast"):
             assert np.array_equal(a, b), (name, comp)
         else:
             scale = max(float(np.abs(b).max()), 1e-300)
