@@ -66,6 +66,7 @@ PHASES = ["control", "reconstruction", "face_flux", "cell_emf", "corner_emf", "u
 # corner_emf, dt | stage 0 update, 2 ghost, colloc_check | 2 x (2 reconstruct,
 # 2 face_flux, cell_emf, corner_emf, update, 2 ghost, colloc_check) | step_end
 LAUNCHES_PER_STEP = 8 + 4 + 2 * 10 + 1
+CPU_SAMPLE_N = 512  # side of the CPU baseline's sample of the workload
 FLOP_PHASE = {"reconstruction": "reconstruction", "face_flux": "face_flux", "cell_emf": "cell_emf",
               "corner_emf": "corner_emf", "update": "update", "collocation": "collocation"}
 
@@ -84,6 +85,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator run")
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-instance batched run")
+    ap.add_argument("--no-other", action="store_true", help="skip the second single-instance case")
     return ap.parse_args()
 
 
@@ -158,9 +160,13 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-def reference_cpu(case, order, steps, warmup, n=128):
+def reference_cpu(case, order, steps, warmup, n=CPU_SAMPLE_N):
     """The reference's own MHD path built for the CPU (oracle/_ref), all host
-    threads, on an n^2 sample of the workload; falls back to the oracle port."""
+    threads, on an n^2 sample of the workload; falls back to the oracle port.
+    Per-zone cost is size-independent on the GPU but not on the CPU (it rises
+    with n up to a few hundred: thread blocks amortise better), so the
+    baseline is sampled at 512^2, the largest size whose steps stay within
+    seconds, and reported per zone."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import mhd_cases as M
     from quasar_b200 import ics
@@ -181,7 +187,8 @@ def reference_cpu(case, order, steps, warmup, n=128):
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": n * n * steps / wall, "unit": "zone-updates/s", "cores": cores, "kind": kind,
             "sample": f"{case} {n}^2 MP{order} outflow, {warmup} untimed + {steps} timed steps "
-                      f"(cfl_limit + step_unchecked), {cores} OpenMP threads"}
+                      f"(cfl_limit + step_unchecked), {cores} OpenMP threads; per-zone rate "
+                      f"extrapolated to the workload's size"}
 
 
 def workload_config(a):
@@ -201,8 +208,9 @@ def run_reference_arm(a):
             "value": cpu["value"], "unit": "zone-updates/s", "n_gpus": a.gpus, "steps": steps,
             "warmup": warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": dict(workload_config(a), sample_n=128,
-                           sample="each step a 128^2 instance of the workload on the host cores"),
+            "config": dict(workload_config(a), sample_n=CPU_SAMPLE_N,
+                           sample=f"each step a {CPU_SAMPLE_N}^2 instance of the workload on the "
+                                  "host cores (per-zone rate)"),
             "cpu_baseline": cpu,
             "e2e": {"value": cpu["value"], "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -235,6 +243,36 @@ def make_batch(insts, order):
         for name, arr in zip(ics_components(), x["arrays"]()):
             b.instance(i).seed_state(name, arr)
     return b
+
+
+def sequential_instances(insts, steps):
+    """Each instance alone, one after another: its own solver's device-timed
+    auto-dt graph loop over `steps` steps after 3 warm-up steps.  Returns
+    (summed device ms, zone-updates)."""
+    import ctypes
+
+    from quasar_b200 import _native, mhd
+    L = _native.lib()
+    ms, done = ctypes.c_double(), ctypes.c_int()
+    total_ms, zu = 0.0, 0
+    for x in insts:
+        c = mhd.MhdConfig()
+        c.grid = mhd.Grid2D(x["nx"], x["ny"], x["lx"], x["ly"])
+        c.reconstruction = "mp5"
+        c.gamma = x["gamma"]
+        side = "periodic" if x["bc"] == 0 else "outflow"
+        c.boundary = mhd.MhdBoundarySpec([side] * 4, [side] * 4)
+        s = mhd.MhdSolver2D(c)
+        for name, arr in zip(ics_components(), x["arrays"]()):
+            s.seed_state(name, arr)
+        for k in (3, steps):
+            _native.check(L.qmhd_solver_time_auto_steps(s._h, k, ctypes.byref(ms), ctypes.byref(done)))
+            if done.value != k:
+                raise RuntimeError(f"sequential instance stopped after {done.value} of {k} steps")
+        total_ms += ms.value
+        zu += x["nx"] * x["ny"] * steps
+        del s
+    return total_ms, zu
 
 
 def ics_components():
@@ -310,6 +348,31 @@ def main():
                 "step_achieved_tflops": (step_flops * value / WORLD / 1e12) if step_flops else None,
                 "phase_ms_per_step": {k: round(v, 4) for k, v in phase_ms.items()}}
 
+    div_b = {"max": s.divergence_b_max(), "rel": s.divergence_b_relative()}
+
+    # the other single-instance workload of the benchmark configuration
+    # (blast beside rotor, same size and order), plain step
+    other = None
+    if not a.no_other:
+        oc = "blast" if a.case == "rotor" else "rotor"
+        # the blast's first steps take positivity retries, which the
+        # graph-only timing loop stops on: run the device-resident loop with
+        # its retry controller (advance_auto) and time it on the host clock
+        so = make_solver(a)
+        seed(so, ics.GENERATORS[oc](a.n, order=a.order))
+        t_sim, _ = so.advance_auto(0.0, float("inf"), max(a.warmup, 3))
+        dist.barrier()
+        w0 = time.perf_counter()
+        t_sim, taken = so.advance_auto(t_sim, float("inf"), a.steps)
+        to = dist.reduce((time.perf_counter() - w0) * 1e3, "max")
+        other = {"workload": f"{oc} {a.n}^2 MP{a.order}, outflow, same step as the headline",
+                 "value": zones * taken * WORLD / (to * 1e-3), "unit": "zone-updates/s",
+                 "ms_per_step": to / max(taken, 1), "steps": taken, "t": t_sim,
+                 "how": "advance_auto (device-resident graph steps plus the positivity "
+                        "controller's retries), host wall clock after warm-up",
+                 "div_b": {"max": so.divergence_b_max(), "rel": so.divergence_b_relative()}}
+        del so
+
     # end to end through the public API with host buffers
     e2e = None
     if not a.no_e2e:
@@ -340,8 +403,11 @@ def main():
         e2e = {"value": zones * k_e2e * WORLD / wall, "unit": "zone-updates/s",
                "h2d_bytes_per_step": bytes_state / k_e2e,
                "d2h_bytes_per_step": bytes_state / k_e2e + 8,
-               "how": "seed_state x8 from pinned host, per step cfl_limit (8-byte dt read back) + "
-                      "step_unchecked, state_component_to_host x8; host wall clock"}
+               "how": "seed_state x8 from pinned host once, then per step cfl_limit (8-byte dt "
+                      "read back) + step_unchecked, then state_component_to_host x8 once: the "
+                      "state crosses PCIe once each way per run of K steps (the reference CLI's "
+                      "seed-once, step-many use), so the per-step bytes are the state / K; "
+                      "host wall clock"}
         del s2
 
     # the same workload with the learned troubled-cell indicator (shipped
@@ -376,7 +442,11 @@ def main():
                    "indicator": f"quasar_b200/data/indicator_mp{a.order}.npz",
                    "threshold": thr, "full_path_face_fraction": (fx + fy) / (2.0 * nfaces),
                    "rho_l1_vs_plain": l1, "steps_compared": max(a.warmup, 3) + a.steps + 1,
-                   "div_b_max": s3.divergence_b_max()}
+                   "div_b_max": s3.divergence_b_max(), "div_b_max_plain": s.divergence_b_max(),
+                   "div_b_rel": s3.divergence_b_relative(),
+                   "div_b_rel_plain": s.divergence_b_relative(),
+                   "div_b_rel_note": "max|div B| dx / max|B_face|, the reference's own measure "
+                                     "(bound 1e-11 in its example tests)"}
         del s3
 
     # batched steps: the 256-instance MP5 batch (plain), and the combined
@@ -384,17 +454,27 @@ def main():
     batched = combined = None
     if not a.no_batch:
         kb = max(10, a.steps // 10)
-        b = make_batch(ics.batch_instances(count=256, seed=0, order=5), 5)
+        insts = ics.batch_instances(count=256, seed=0, order=5)
+        b = make_batch(insts, 5)
         ctas, trials = b.autotune()
         b.time_steps(3)
         bms, bzu = b.time_steps(kb)
         bms = dist.reduce(bms, "max")
+        del b
+        seq_ms, seq_zu = sequential_instances(insts, kb)
+        seq_ms = dist.reduce(seq_ms, "max")
         batched = {"workload": "256 seeded MP5 instances, sides log-uniform in [64, 512], "
                                "Orszag-Tang / oblique Brio-Wu / linear fast or Alfven waves",
-                   "zones": b.zones(), "value": bzu * WORLD / (bms * 1e-3), "unit": "zone-updates/s",
+                   "zones": sum(x["nx"] * x["ny"] for x in insts),
+                   "value": bzu * WORLD / (bms * 1e-3), "unit": "zone-updates/s",
                    "ms_per_step": bms / kb, "autotuned_ctas_per_sm": ctas,
-                   "autotune_steps": trials}
-        del b
+                   "autotune_steps": trials,
+                   "sequential": {"value": seq_zu * WORLD / (seq_ms * 1e-3),
+                                  "ms_per_step": seq_ms / kb,
+                                  "how": "the same instances stepped one after another, each "
+                                         "its own solver's device-resident graph loop of the "
+                                         "same steps, device times summed"},
+                   "batch_over_sequential": (bzu / bms) / (seq_zu / seq_ms)}
         if not a.no_learned:
             from quasar_b200 import train_indicator
             from quasar_b200.indicator import attach_batch
@@ -421,7 +501,9 @@ def main():
 
     cpu = None
     if RANK == 0 and WORLD == 1 and not a.no_cpu:
-        cpu = reference_cpu(a.case, a.order, 3, 1)
+        cpu = reference_cpu(a.case, a.order, 2, 1)
+        small = reference_cpu(a.case, a.order, 3, 1, n=128)
+        cpu["small_sample"] = {"value": small["value"], "sample": small["sample"]}
 
     if RANK == 0:
         line = {"metric": "MHD zone-updates/s (plain FP64 step)", "value": value,
@@ -431,6 +513,7 @@ def main():
                 "config": workload_config(a),
                 "gpu_launches": LAUNCHES_PER_STEP * a.steps,
                 "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "div_b": div_b, "other_case": other,
                 "learned": learned, "batched": batched, "batched_learned": combined}
         print(json.dumps(line), flush=True)
     dist.close()

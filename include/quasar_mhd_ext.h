@@ -46,11 +46,16 @@ int qmhd_fp64_fma_peak(double* tflops);
  * unless an error message is formatted.  nx*ny above
  * QMHD_TOTALS_DEVICE_MAX_CELLS returns QMHD_INVALID_ARGUMENT.  No part of the
  * scratch has to start at zero: each call writes every slot it reads.
- * The first call on each device looks up the scratch address (a
- * cudaGetSymbolAddress); make that first call before any stream capture
- * begins on the device.  Calls on one device share the one scratch array, so
- * overlapping calls (other threads, or streams running at once) race and must
- * be serialised by the caller. */
+ * rho and energy must be device or managed memory whose device is the
+ * current one (managed memory whose device is another GPU is rejected).
+ * Every call looks up the scratch address in the current context (a
+ * cudaGetSymbolAddress, which allocates nothing), so a cudaDeviceReset
+ * between calls is harmless.  Calls on one device share the one scratch
+ * array: they hold a per-device lock from the lookup until their stream has
+ * synchronized, so calls from several host threads take turns and never
+ * overlap on the GPU (other processes have their own copy of the array).
+ * Every call copies to pageable host memory and synchronizes its stream, so
+ * it must not be made while any stream capture is active on the device. */
 int qmhd_conserved_cell_totals_device(const double* rho, const double* energy, int nx, int ny,
                                       int nghost, void* stream, double* mass,
                                       double* energy_total);

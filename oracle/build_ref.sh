@@ -12,7 +12,10 @@
 # (scaled_arithmetic.hpp:22-23); x86-64 g++ emits no FMA contraction anyway.
 set -euo pipefail
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${REF:-/root/reference}
+if [ -z "${REF:-}" ]; then
+  echo "$(basename "$0"): set REF to the quasar source tree" >&2
+  exit 2
+fi
 OUT=$HERE/_ref
 OBJ=$OUT/obj
 if [ ! -d "$REF/src/backend/hip/mhd" ]; then

@@ -13,7 +13,10 @@
 set -euo pipefail
 HERE=$(cd "$(dirname "$0")" && pwd)
 ROOT=$(cd "$HERE/.." && pwd)
-REF=${REF:-/root/reference}
+if [ -z "${REF:-}" ]; then
+  echo "$(basename "$0"): set REF to the quasar source tree" >&2
+  exit 2
+fi
 CUDA=${CUDA_HOME:-/usr/local/cuda}
 OUT=$HERE/_ref
 OBJ=$OUT/obj_seam

@@ -444,8 +444,8 @@ int qmhd_solver_learned_face_counts(qmhd_solver* solver, long long* x_faces, lon
   });
 }
 
-// Allocation-free totals over caller-owned device arrays: validation, the
-// once-per-device scratch lookup, then the two reductions.  Returns codes
+// Allocation-free totals over caller-owned device arrays: validation, then
+// the scratch lookup and the two reductions under the device's lock.  Returns codes
 // directly (no exceptions) so the success path allocates nothing on the host.
 static_assert(QMHD_TOTALS_DEVICE_MAX_CELLS == qb::kTotalsMaxCells, "scratch limit");
 
@@ -495,19 +495,10 @@ int qmhd_conserved_cell_totals_device(const double* rho, const double* energy, i
       return fail(QMHD_INVALID_ARGUMENT);
     }
   }
-  double* scratch = nullptr;
-  rc = qb::totals_scratch(device, &scratch);
-  if (rc != cudaSuccess) {
-    std::snprintf(msg, sizeof msg,
-                  "qmhd_conserved_cell_totals_device: scratch lookup on device %d: %s", device,
-                  cudaGetErrorString(rc));
-    return fail(QMHD_DEVICE_ERROR);
-  }
   double totals[2];
-  rc = qb::launch_totals_noalloc(rho, energy, nx, ny, nghost, scratch, (cudaStream_t)stream,
-                                 totals);
+  rc = qb::totals_noalloc(device, rho, energy, nx, ny, nghost, (cudaStream_t)stream, totals);
   if (rc != cudaSuccess) {
-    std::snprintf(msg, sizeof msg, "qmhd_conserved_cell_totals_device: %s",
+    std::snprintf(msg, sizeof msg, "qmhd_conserved_cell_totals_device: device %d: %s", device,
                   cudaGetErrorString(rc));
     return fail(QMHD_DEVICE_ERROR);
   }

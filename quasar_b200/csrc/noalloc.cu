@@ -20,8 +20,10 @@ constexpr int kThreads = 256;
 // call, so nothing here has to start at zero.
 static __device__ __align__(256) double g_totals_scratch[4 * kTotalsMaxPartials + 2];
 
-std::mutex g_setup_mu;
-double* g_scratch_ptr[kTotalsMaxDevices] = {};
+// One lock per device, held from the scratch lookup until the stream has
+// synchronized: calls from different host threads on one device take turns
+// instead of sharing the scratch array at the same time.
+std::mutex g_device_mu[kTotalsMaxDevices];
 
 // s + v with its rounding error added to c (Knuth's TwoSum, no contraction).
 __device__ __forceinline__ void comp_add(double& s, double& c, double v) {
@@ -94,22 +96,16 @@ k_sum_partials(const double* __restrict__ partial, int parts, double* __restrict
 
 }  // namespace
 
-// Address of this device's scratch, looked up once per device under a lock.
-cudaError_t totals_scratch(int device, double** ptr) {
+cudaError_t totals_noalloc(int device, const double* rho, const double* energy, int nx, int ny,
+                          int ng, cudaStream_t stream, double totals[2]) {
   if (device < 0 || device >= kTotalsMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_scratch_ptr[device]) {
-    double* p = nullptr;
-    const cudaError_t rc = cudaGetSymbolAddress((void**)&p, g_totals_scratch);
-    if (rc != cudaSuccess) return rc;
-    g_scratch_ptr[device] = p;
-  }
-  *ptr = g_scratch_ptr[device];
-  return cudaSuccess;
-}
-
-cudaError_t launch_totals_noalloc(const double* rho, const double* energy, int nx, int ny, int ng,
-                                  double* scratch, cudaStream_t stream, double totals[2]) {
+  std::lock_guard<std::mutex> lock(g_device_mu[device]);
+  // The symbol's address is looked up on every call (it allocates nothing),
+  // so it always belongs to the context that is current now, also after a
+  // cudaDeviceReset.
+  double* scratch = nullptr;
+  cudaError_t rc = cudaGetSymbolAddress((void**)&scratch, g_totals_scratch);
+  if (rc != cudaSuccess) return rc;
   const long long cells = (long long)nx * ny;
   const int parts = int((cells + kTotalsChunk - 1) / kTotalsChunk);
   double* partial = scratch;
@@ -117,7 +113,7 @@ cudaError_t launch_totals_noalloc(const double* rho, const double* energy, int n
   k_cell_sums_chunk<<<parts, kThreads, 0, stream>>>(rho, energy, nx, cells, ng,
                                                     (long long)nx + 2 * ng, partial);
   k_sum_partials<<<1, kThreads, 0, stream>>>(partial, parts, result);
-  cudaError_t rc = cudaGetLastError();
+  rc = cudaGetLastError();
   if (rc != cudaSuccess) return rc;
   rc = cudaMemcpyAsync(totals, result, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream);
   if (rc != cudaSuccess) return rc;

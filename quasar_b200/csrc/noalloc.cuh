@@ -9,13 +9,11 @@ constexpr int kTotalsMaxPartials = 8192;      // scratch: 8192 x 4 doubles (256 
 constexpr long long kTotalsMaxCells = kTotalsChunk * kTotalsMaxPartials;  // 67,108,864
 constexpr int kTotalsMaxDevices = 64;
 
-// Device address of the static scratch on `device` (the calling thread's
-// current device); the lookup runs once per device.
-cudaError_t totals_scratch(int device, double** ptr);
-
-// Launch the chunked sums and the final reduction on `stream`, copy the two
-// totals to host and synchronize the stream.  Sizes must already be checked.
-cudaError_t launch_totals_noalloc(const double* rho, const double* energy, int nx, int ny, int ng,
-                                  double* scratch, cudaStream_t stream, double totals[2]);
+// Under a per-device lock: look up the static scratch's address in the
+// current context, launch the chunked sums and the final reduction on
+// `stream`, copy the two totals to host and synchronize the stream.  `device`
+// is the calling thread's current device; sizes must already be checked.
+cudaError_t totals_noalloc(int device, const double* rho, const double* energy, int nx, int ny,
+                          int ng, cudaStream_t stream, double totals[2]);
 
 }  // namespace qb

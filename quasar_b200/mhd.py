@@ -219,6 +219,20 @@ class MhdSolver2D:
         _native.check(_native.lib().qmhd_solver_divergence_b_max(self._h, ctypes.byref(d)))
         return d.value
 
+    def divergence_b_relative(self) -> float:
+        """Dimensionless solenoidality: max |div B| x dx / max |B_face| over
+        the evolved faces, the measure the reference's own example tests
+        assert (tests/python/test_examples.py:1985-2003: below 1e-11).  Not a
+        method of the reference's solver; it reads the face field back."""
+        g = self._grid
+        ng, nx, ny = g.nghost, g.nx, g.ny
+        shape = (ny + 2 * ng, nx + 2 * ng)
+        bx = self.state_component_to_host("bx_face").reshape(shape)[ng:ng + ny, ng:ng + nx + 1]
+        by = self.state_component_to_host("by_face").reshape(shape)[ng:ng + ny + 1, ng:ng + nx]
+        bmax = float(max(np.abs(bx).max(), np.abs(by).max()))
+        d = self.divergence_b_max()
+        return d * g.dx() / bmax if bmax > 0.0 else d
+
     def conserved_cell_totals(self):
         m, e = ctypes.c_double(), ctypes.c_double()
         _native.check(_native.lib().qmhd_solver_conserved_cell_totals(

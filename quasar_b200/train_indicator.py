@@ -138,7 +138,9 @@ def inference_report(n=2048, order=5, t_develop=0.3, steps=100, snapshots=2, pat
             "limiter_recall": ev["recall"], "cells_flagged": ev["flagged"],
             "label_tol": tol, "labelled_cells": ev["total"], "limiter_positive": ev["positives"],
             "full_path_face_fraction": float(np.mean(face_frac)),
-            "div_b_max": learned.divergence_b_max()}
+            "div_b_max": learned.divergence_b_max(), "div_b_max_plain": plain.divergence_b_max(),
+            "div_b_rel": learned.divergence_b_relative(),
+            "div_b_rel_plain": plain.divergence_b_relative()}
 
 
 def default_path(order):

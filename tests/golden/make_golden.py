@@ -3,10 +3,15 @@ MHD solver built for the CPU (oracle/build_ref.sh -> oracle/_ref).
 
     python tests/golden/make_golden.py short     # few-step fixtures (seconds)
     python tests/golden/make_golden.py ot_t05    # OT 128^2 MP5 to t=0.5 (long)
+    python tests/golden/make_golden.py large     # rotor / blast 512^2 MP7 (minutes)
 
 Fixtures hold the seeded initial state's generator parameters, the dt of
 every step and the reference state after the last step, so GPU tests can pin
 the CUDA product against the reference where the reference itself cannot run.
+The 512^2 fixtures (the benchmark's rotor and blast workloads at MP7) keep
+the state in summary form to stay small: per component, over its evolved
+region, the signed and absolute sums of every row and column, and every 8th
+value of every 8th row.
 """
 from __future__ import annotations
 
@@ -30,6 +35,28 @@ SHORT = [
     ("ot24_muscl", "ot", 24, 2, M.PERIODIC, 5),
 ]
 CASES = {"ot": M.orszag_tang, "rotor": M.rotor, "blast": M.blast}
+
+
+LARGE = [
+    ("rotor512_mp7", "rotor", 512, 7, M.OUTFLOW, 2),
+    ("blast512_mp7", "blast", 512, 7, M.OUTFLOW, 2),
+]
+SUB = 8  # subsample stride of the summary fixtures
+
+
+def summarize(st, ng, n):
+    """Per component, over its evolved region (interior cells, plus the owned
+    high faces of the face fields): signed and absolute sums of every row and
+    column, and every SUB-th value of every SUB-th row."""
+    out = {}
+    for c, name in enumerate(M.COMPONENTS):
+        a = M._evolved(st[c], c, ng, n, n)
+        out[name + "_row_sum"] = a.sum(axis=1)
+        out[name + "_row_abs"] = np.abs(a).sum(axis=1)
+        out[name + "_col_sum"] = a.sum(axis=0)
+        out[name + "_col_abs"] = np.abs(a).sum(axis=0)
+        out[name + "_sub"] = a[::SUB, ::SUB].copy()
+    return out
 
 
 def run(name, case, n, order, bc, steps=None, t_end=None, keep="all"):
@@ -56,9 +83,12 @@ def run(name, case, n, order, bc, steps=None, t_end=None, keep="all"):
     st = s.read()
     d = ctypes_divb(R, s)
     payload = dict(case=case, n=n, order=order, bc=np.array(bc), dts=np.array(dts), t=t, divb=d)
-    comps = range(8) if keep == "all" else [0]
-    for c in comps:
-        payload[M.COMPONENTS[c]] = st[c]
+    if keep == "summary":
+        payload.update(summarize(st, M.nghost(order), n), sub_stride=SUB)
+    else:
+        comps = range(8) if keep == "all" else [0]
+        for c in comps:
+            payload[M.COMPONENTS[c]] = st[c]
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **payload)
     print(f"{name}: {k} steps t={t:.6g} divb={d:.3e} ({time.time() - t0:.1f}s)")
 
@@ -77,3 +107,6 @@ if __name__ == "__main__":
             run(*row)
     elif what == "ot_t05":
         run("ot128_mp5_t05", "ot", 128, 5, M.PERIODIC, t_end=0.5, keep="rho")
+    elif what == "large":
+        for row in LARGE:
+            run(*row, keep="summary")

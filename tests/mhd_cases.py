@@ -272,6 +272,33 @@ def state_rel_l1(sa, sb, ng, nx, ny):
     return worst
 
 
+def summary_rel(state, fx, n, order):
+    """Largest relative L1 gap, per physical group, between a state and a
+    summary fixture (tests/golden/make_golden.py `summarize`): over the
+    strided subsample, the row sums and the column sums.  A cell that
+    differs shows in its row's and its column's sum (and in the subsample
+    when it lies on the stride), so a local defect cannot hide."""
+    ng = nghost(order)
+    sub = int(fx["sub_stride"])
+    worst = 0.0
+    for grp in GROUPS:
+        num = {"sub": 0.0, "row": 0.0, "col": 0.0}
+        den = dict(num)
+        for c in grp:
+            name = COMPONENTS[c]
+            a = _evolved(state[c], c, ng, n, n)
+            num["sub"] += np.abs(a[::sub, ::sub] - fx[name + "_sub"]).sum()
+            den["sub"] += np.abs(fx[name + "_sub"]).sum()
+            num["row"] += np.abs(a.sum(axis=1) - fx[name + "_row_sum"]).sum()
+            den["row"] += fx[name + "_row_abs"].sum()
+            num["col"] += np.abs(a.sum(axis=0) - fx[name + "_col_sum"]).sum()
+            den["col"] += fx[name + "_col_abs"].sum()
+        for k in num:
+            if num[k] > 0.0:
+                worst = max(worst, num[k] / den[k] if den[k] > 0.0 else np.inf)
+    return worst
+
+
 def divb_max(s, ng, nx, ny, dx, dy):
     bx, by = s[5], s[6]
     d = ((bx[ng:ng + ny, ng + 1:ng + nx + 1] - bx[ng:ng + ny, ng:ng + nx]) / dx +

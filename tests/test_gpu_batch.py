@@ -126,6 +126,9 @@ def test_oblique_families_match_oracle(oracle, family):
     assert g.divergence_b_max() <= 1e-12
 
 
+DIVB_NOISE = 2.0  # spread of two round-off random walks of the same statistics
+
+
 def _seeded_pair(order, count, seed):
     insts = mixed_instances(order, count=count, seed=seed)
     b = mhd.MhdBatch2D([config(x, order) for x in insts])
@@ -166,4 +169,10 @@ def test_batched_learned_with_shipped_indicator_stays_close():
         rc = read_all(c.instance(i), x, order)[0][ng:-ng, ng:-ng]
         l1 = np.sum(np.abs(rc - rb)) / np.sum(np.abs(rb))
         assert l1 <= 1e-4, (x["family"], i, l1)
-        assert c.instance(i).divergence_b_max() <= 1e-11
+        # solenoidality in the reference's relative measure and bound
+        # (tests/python/test_examples.py:1985-2003), and at the plain run's
+        # own round-off level: CT keeps div B exact in exact arithmetic for
+        # any EMF, so both runs carry a random walk of the same rounding
+        # statistics (DIVB_NOISE allows for its spread)
+        rel_l, rel_p = c.instance(i).divergence_b_relative(), b.instance(i).divergence_b_relative()
+        assert rel_l < 1e-11 and rel_l <= DIVB_NOISE * max(rel_p, 1e-15), (x["family"], i, rel_l, rel_p)

@@ -132,4 +132,8 @@ def test_inference_report_on_developed_orszag_tang():
     assert r["rho_l1_vs_plain"] <= 1e-4
     assert r["limiter_recall"] >= 0.8
     assert r["cells_flagged"] < 0.35 and r["full_path_face_fraction"] < 0.35
-    assert r["div_b_max"] <= 1e-10
+    # solenoidality in the reference's relative measure and bound
+    # (tests/python/test_examples.py:1985-2003), at the plain run's own
+    # round-off level (both are random walks of the same rounding statistics)
+    assert r["div_b_rel"] < 1e-11, r
+    assert r["div_b_rel"] <= 2.0 * max(r["div_b_rel_plain"], 1e-15), r

@@ -136,7 +136,11 @@ def test_reductions_match_solver(case, n, order, bc):
     assert cfl_eff / rate.scaled_max_rate == s.cfl_limit()
     assert L.ct_divb_linf(w.grid, U0, w.scratch) == s.divergence_b_max()
     assert L.ct_divb_relative_linf(w.grid, U0, w.scratch) <= 1024 * np.finfo(float).eps
-    assert L.conserved_cell_sums(w.grid, U0) == s.conserved_cell_totals()
+    # the launch form sums 8192-cell chunks on the device, the solver's
+    # totals finish its block partials on the host: two summation orders of
+    # compensated sums, equal to a few ulp
+    for got, want in zip(L.conserved_cell_sums(w.grid, U0), s.conserved_cell_totals()):
+        assert abs(got - want) <= 1e-13 * abs(want), (got, want)
     assert L.admissible_fraction(w.grid, U0, U0, 0.0, 0.0, GAMMA, w.scratch) == 1.0
     # one cell of the candidate with its density negated: the edge of the
     # admissible segment is that cell's, found by the bisection restated here

@@ -72,6 +72,28 @@ def test_steps_match_oracle_and_reference(oracle, name):
     assert g.divergence_b_max() <= 1e-12
 
 
+@pytest.mark.parametrize("name", ["rotor512_mp7", "blast512_mp7"])
+def test_benchmark_workloads_512_match_reference(name):
+    """The benchmark's workloads (MHD rotor and blast, MP7, outflow) at 512^2,
+    two steps against the reference's own solver (summary fixtures made by
+    tests/golden/make_golden.py large): dt within 1e-12, the state within
+    1e-10 relative L1 per step, div B at round-off."""
+    fx = load_fixture(name)
+    n, order, case = int(fx["n"]), int(fx["order"]), str(fx["case"])
+    bc = tuple(int(b) for b in fx["bc"])
+    g = gpu_solver(n, order, bc)
+    seed(g, CASES[case](n, order=order))
+    for k, dt_ref in enumerate(fx["dts"]):
+        dt = g.cfl_limit()
+        assert abs(dt - dt_ref) <= DT_TOL * dt_ref, (k, dt, dt_ref)
+        g.step_unchecked(dt_ref)
+    ng = M.nghost(order)
+    state = read(g, (n + 2 * ng, n + 2 * ng))
+    err = M.summary_rel(state, fx, n, order)
+    assert err <= STEP_TOL * len(fx["dts"]), err
+    assert g.divergence_b_max() <= 1e-12
+
+
 def test_divb_roundoff_and_conservation():
     n, order = 64, 5
     g = gpu_solver(n, order)

@@ -35,6 +35,21 @@ def test_oracle_matches_reference_fixture(oracle, name):
     assert M.state_rel_l1(got, want, s.ng, n, n) <= 1e-13
 
 
+@pytest.mark.parametrize("name", ["rotor512_mp7", "blast512_mp7"])
+def test_oracle_matches_reference_at_benchmark_workloads_512(oracle, name):
+    """The benchmark's rotor and blast MP7 workloads at 512^2: two steps of
+    the oracle against the reference's summary fixtures."""
+    fx = load_fixture(name)
+    n, order, case = int(fx["n"]), int(fx["order"]), str(fx["case"])
+    s = oracle.solver(n, n, order, bc=tuple(int(b) for b in fx["bc"]))
+    s.seed(CASES[case](n, order=order))
+    for k, dt_ref in enumerate(fx["dts"]):
+        dt = s.cfl()
+        assert abs(dt - dt_ref) <= 1e-13 * dt_ref, (k, dt, dt_ref)
+        s.step(dt_ref)
+    assert M.summary_rel(s.read(), fx, n, order) <= 1e-13
+
+
 def test_oracle_residual_matches_reference(oracle, ref):
     n, order = 24, 7
     ic = M.rotor(n, order=order)
