@@ -275,41 +275,29 @@ __device__ __forceinline__ double mp_limit(double vl, double vm2, double vm1, do
   const double vmax = fmin(fmax(fmax(v0, vp1), v_md), fmax(fmax(v0, v_ul), v_lc));
   return vl + minmod2(vmin - vl, vmax - vl);
 }
-// mp_limiter.hpp:182-224: W = 5 (MP5) or 7 (MP7); v[0..W-1].  The stencil is
-// normalised by its largest magnitude through one reciprocal.
-// Unlimited MP interpolation of the W-point stencil v[] to the face:
-// normalised by the stencil's largest magnitude through one reciprocal.
-template <int W>
-__device__ __forceinline__ double mp_interp(const double* v) {
-  double s = 0.0;
-#pragma unroll
-  for (int k = 0; k < W; ++k) s = fmax(s, fabs(v[k]));
-  if (s == 0.0) return 0.0;
-  const double is = 1.0 / s;
-  if (W == 5) {
-    const double sum = 2.0 * (v[0] * is) - 13.0 * (v[1] * is) + 47.0 * (v[2] * is) +
-                       27.0 * (v[3] * is) - 3.0 * (v[4] * is);
-    return (sum * (1.0 / 60.0)) * s;
-  }
-  const double sum = -3.0 * (v[0] * is) + 25.0 * (v[1] * is) - 101.0 * (v[2] * is) +
-                     319.0 * (v[3] * is) + 214.0 * (v[4] * is) - 38.0 * (v[5] * is) +
-                     4.0 * (v[6] * is);
-  return (sum * (1.0 / 420.0)) * s;
-}
-
-// The same interpolation without the magnitude normalisation (the
-// component-wise fast path, where overflow guarding is not needed).
+// mp_limiter.hpp:182-224: the unlimited MP interpolation of the W-point
+// stencil v[0..W-1] to the face, W = 5 (MP5) or 7 (MP7).  The reference
+// divides every term by the stencil's largest magnitude first, which only
+// guards binary64 overflow for values near 1e305 (outside every
+// configuration here); the weights are applied directly, summed as a shallow
+// tree (two-term FMA pairs) rather than one dependent chain, a
+// rounding-level difference.
 template <int W>
 __device__ __forceinline__ double mp_interp_plain(const double* v) {
-  if (W == 5)
-    return (2.0 * v[0] - 13.0 * v[1] + 47.0 * v[2] + 27.0 * v[3] - 3.0 * v[4]) * (1.0 / 60.0);
-  return (-3.0 * v[0] + 25.0 * v[1] - 101.0 * v[2] + 319.0 * v[3] + 214.0 * v[4] - 38.0 * v[5] +
-          4.0 * v[6]) * (1.0 / 420.0);
+  if (W == 5) {
+    const double a = fma(-13.0, v[1], 2.0 * v[0]);
+    const double b = fma(27.0, v[3], 47.0 * v[2]);
+    return ((a + b) + (-3.0 * v[4])) * (1.0 / 60.0);
+  }
+  const double a = fma(25.0, v[1], -3.0 * v[0]);
+  const double b = fma(319.0, v[3], -101.0 * v[2]);
+  const double c = fma(-38.0, v[5], 214.0 * v[4]);
+  return ((a + b) + (c + 4.0 * v[6])) * (1.0 / 420.0);
 }
 
 template <int W>
 __device__ __forceinline__ double mp_recon(const double* v, bool& fired) {
-  const double vl = mp_interp<W>(v);
+  const double vl = mp_interp_plain<W>(v);
   constexpr int o = W == 5 ? 0 : 1;
   return mp_limit(vl, v[o], v[o + 1], v[o + 2], v[o + 3], v[o + 4], fired);
 }

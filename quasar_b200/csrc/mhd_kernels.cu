@@ -700,6 +700,325 @@ __device__ void mp_pair_lin(const StateP& u, long long k0, long long step, St& u
   ur = rot<DIR>(sr);
 }
 
+template <int DIR, int ORDER, int MODE>
+__device__ __forceinline__ void finish_face(const Grid& g, const StateP& u, const IfaceP& out,
+                                            double gamma, int i, int j, long long k0,
+                                            long long step, St ul, St ur);
+
+// ---- warp-cooperative characteristic MP reconstruction --------------------
+// The characteristic path of mp_pair_loop with the work of one face spread
+// over four lanes, lane r holding the pair of waves r and 6 - r (lane 3 the
+// entropy wave alone), so that a thread carries two waves' L rows and
+// projected stencils instead of all seven, and has two independent chains.
+// A warp owns 32 faces:
+//   phase 1  lane = face: reference state and eigen scalars -> shared memory
+//   phase 2  4 rounds of 8 faces, lane = (face, wave pair): L rows and R
+//            columns, the L R = I check (R columns exchanged through shared
+//            memory), the stencil deltas (lane = two stencil cells),
+//            projection, MP limiter on both sides, back-projection (lane =
+//            components r and r + 4)
+//   phase 3  lane = face: states, fallback chain, stores (finish_face)
+// Every value is formed by the same operations in the same order as
+// mp_pair_loop, so the two paths agree to the FMA contraction the compiler
+// picks for each expression.  Four lanes per face (not seven) because the
+// exchanged operands are read once per lane: each shared-memory load costs
+// one wavefront per half-warp whether or not the lanes share its address.
+//
+// Per-warp shared memory (doubles): a face record [kRec][32] and eight group
+// buffers R[7][7] followed by delta[8][7], whose first 14 slots later hold
+// the projected face values w[2][7].
+constexpr int kRecC = 0;    // canonical reference state, 8 components
+constexpr int kRecE = 8;    // 17 eigen scalars, later dl[7] and dr[7]
+constexpr int kRec = 25;
+constexpr int kGrpR = 0, kGrpD = 49, kGrpW = 49, kGrpDoubles = 105;
+constexpr int kGroups = 8;
+constexpr int kWarpReconDoubles = kRec * 32 + kGroups * kGrpDoubles;
+constexpr int kReconWarps = 4;
+constexpr size_t kReconWarpSmem = size_t(kReconWarps) * kWarpReconDoubles * sizeof(double);
+
+// L row and R column of wave k (k = 7: zeros) without branching on k: the
+// three families are formed side by side and selected, entry for entry the
+// products of wave_vectors and the sums of conserved_row_col.
+__device__ __forceinline__ void wave_lr(const Eg& e, int k, double* Lr, double* Rc) {
+  const double rho = e.rho;
+  const double s2 = kRs2, Nf = 0.5 * e.ia2;
+  // magnetosonic (k = 0, 2, 4, 6): fast for 0 and 6, slow for 2 and 4;
+  // the "minus" member of each pair is k < 3
+  const bool fs = (k == 0 || k == 6);
+  const bool neg = k < 3;
+  const double qf = e.cf * e.af * e.sbn, qs = e.cs * e.as * e.sbn;
+  const double Af = e.a * e.af * e.sr, As = e.a * e.as * e.sr;
+  const double al = fs ? e.af : e.as;
+  const double cc = fs ? e.cf : e.cs;
+  const double qq = fs ? qs : -qf;
+  const double AA = fs ? As : -Af;
+  const double ac = al * cc, qb1 = qq * e.b1, qb2 = qq * e.b2;
+  const double nac = Nf * al * cc, nq1 = Nf * qq * e.b1, nq2 = Nf * qq * e.b2;
+  // Alfven (k = 1, 5): the "minus" member is k = 1
+  const double t5 = e.sbn * e.b2 * s2 * e.sr, t6 = e.sbn * e.b1 * s2 * e.sr;
+  const double u5 = e.sbn * e.b2 * s2 * e.isr, u6 = e.sbn * e.b1 * s2 * e.isr;
+  const double ab2 = -e.b2 * s2, ab1 = e.b1 * s2;
+  const bool ms = (k & 1) == 0 && k != 7, alf = k == 1 || k == 5, ent = k == 3;
+  const bool k1 = k == 1;
+  double rp[7], lp[7];
+  rp[0] = ms ? rho * al : (ent ? 1.0 : 0.0);
+  rp[1] = ms ? (neg ? -ac : ac) : 0.0;
+  rp[2] = ms ? (neg ? qb1 : -qb1) : (alf ? ab2 : 0.0);
+  rp[3] = ms ? (neg ? qb2 : -qb2) : (alf ? ab1 : 0.0);
+  rp[4] = ms ? al * e.ra2 : 0.0;
+  rp[5] = ms ? AA * e.b1 : (alf ? (k1 ? -t5 : t5) : 0.0);
+  rp[6] = ms ? AA * e.b2 : (alf ? (k1 ? t6 : -t6) : 0.0);
+  lp[0] = ent ? 1.0 : 0.0;
+  lp[1] = ms ? (neg ? -nac : nac) : 0.0;
+  lp[2] = ms ? (neg ? nq1 : -nq1) : (alf ? ab2 : 0.0);
+  lp[3] = ms ? (neg ? nq2 : -nq2) : (alf ? ab1 : 0.0);
+  lp[4] = ms ? Nf * al * e.ir : (ent ? -e.ia2 : 0.0);
+  lp[5] = ms ? Nf * AA * e.b1 * e.ir : (alf ? (k1 ? -u5 : u5) : 0.0);
+  lp[6] = ms ? Nf * AA * e.b2 * e.ir : (alf ? (k1 ? u6 : -u6) : 0.0);
+  const double gv = e.gm1;
+  Lr[0] = (((lp[0] * 1.0 + lp[1] * (-e.vn * e.ir)) + lp[2] * (-e.vt1 * e.ir)) +
+           lp[3] * (-e.vt2 * e.ir)) + lp[4] * (gv * e.hv2);
+  Lr[1] = lp[1] * e.ir + lp[4] * (-gv * e.vn);
+  Lr[2] = lp[2] * e.ir + lp[4] * (-gv * e.vt1);
+  Lr[3] = lp[3] * e.ir + lp[4] * (-gv * e.vt2);
+  Lr[4] = lp[4] * gv;
+  Lr[5] = lp[4] * (-gv * e.bt1) + lp[5];
+  Lr[6] = lp[4] * (-gv * e.bt2) + lp[6];
+  Rc[0] = rp[0];
+  Rc[1] = e.vn * rp[0] + e.rho * rp[1];
+  Rc[2] = e.vt1 * rp[0] + e.rho * rp[2];
+  Rc[3] = e.vt2 * rp[0] + e.rho * rp[3];
+  Rc[4] = (((((e.hv2 * rp[0] + (e.rho * e.vn) * rp[1]) + (e.rho * e.vt1) * rp[2]) +
+             (e.rho * e.vt2) * rp[3]) + e.igm * rp[4]) + e.bt1 * rp[5]) + e.bt2 * rp[6];
+  Rc[5] = rp[5];
+  Rc[6] = rp[6];
+}
+
+// One warp's 32 faces (lane = face; `valid` false for lanes without one).
+// All lanes of the warp must call it; `ws` is the warp's shared memory.
+template <int DIR, int ORDER>
+__device__ void mp_faces_warp(const Grid& g, const StateP& u, const IfaceP& out, double gamma,
+                              int i, int j, bool valid, double* ws) {
+  constexpr int H = ORDER == 5 ? 2 : 3;
+  constexpr int S = 2 * H + 2, W = 2 * H + 1;
+  const unsigned lane = threadIdx.x & 31u;
+  const long long step = DIR == 0 ? 1 : g.pitch;
+  const long long k0 = valid ? g.idx(i, j) : 0;
+  double* rec = ws;
+  // phase 1: reference state and eigen scalars of this lane's face
+  if (valid) {
+    const St cl = load_cell(u, k0 - step), cr = load_cell(u, k0);
+    St ref;
+    ref.rho = 0.5 * cl.rho + 0.5 * cr.rho;
+    ref.mx = 0.5 * cl.mx + 0.5 * cr.mx;
+    ref.my = 0.5 * cl.my + 0.5 * cr.my;
+    ref.mz = 0.5 * cl.mz + 0.5 * cr.mz;
+    ref.E = 0.5 * cl.E + 0.5 * cr.E;
+    ref.bx = 0.5 * cl.bx + 0.5 * cr.bx;
+    ref.by = 0.5 * cl.by + 0.5 * cr.by;
+    ref.bz = 0.5 * cl.bz + 0.5 * cr.bz;
+    const St c = rot<DIR>(ref);
+    const Eg e = eig_scalars(c, gamma);
+    double* r = rec + lane;
+    r[(kRecC + 0) * 32] = c.rho;
+    r[(kRecC + 1) * 32] = c.mx;
+    r[(kRecC + 2) * 32] = c.my;
+    r[(kRecC + 3) * 32] = c.mz;
+    r[(kRecC + 4) * 32] = c.E;
+    r[(kRecC + 5) * 32] = c.bx;
+    r[(kRecC + 6) * 32] = c.by;
+    r[(kRecC + 7) * 32] = c.bz;
+    const double ev[17] = {e.sr, e.cf, e.cs, e.a, e.af, e.as, e.b1, e.b2, e.sbn,
+                           e.vn, e.vt1, e.vt2, e.ia2, e.ra2, e.hv2, e.ir, e.isr};
+#pragma unroll
+    for (int q = 0; q < 17; ++q) r[(kRecE + q) * 32] = ev[q];
+  }
+  const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+  // phase 2: eight faces per round, four lanes per face
+  const int gi = int(lane >> 2), rl = int(lane & 3u);
+  const bool two = rl < 3;           // lanes 0-2: waves rl and 6 - rl; lane 3: wave 3
+  const int ka = rl, kb = 6 - rl;    // kb == ka on lane 3
+  double* grp = ws + kRec * 32 + gi * kGrpDoubles;
+  const double gm1 = gamma - 1.0, igm = 1.0 / gm1;
+  constexpr double kT2 = (1024.0 * kEps) * (1024.0 * kEps);
+#pragma unroll 1
+  for (int rd = 0; rd < 4; ++rd) {
+    if (((vmask >> (8 * rd)) & 0xFFu) == 0u) continue;  // warp-uniform
+    const int f = 8 * rd + gi;
+    const bool on = (vmask >> f) & 1u;
+    const long long kf = __shfl_sync(0xffffffffu, k0, f);
+    double La[7], Lb[7];
+    bool ok = true;
+    if (on) {
+      const double* r = rec + f;
+      Eg e;
+      e.rho = r[(kRecC + 0) * 32];
+      e.bt1 = r[(kRecC + 6) * 32];
+      e.bt2 = r[(kRecC + 7) * 32];
+      e.sr = r[(kRecE + 0) * 32];
+      e.cf = r[(kRecE + 1) * 32];
+      e.cs = r[(kRecE + 2) * 32];
+      e.a = r[(kRecE + 3) * 32];
+      e.af = r[(kRecE + 4) * 32];
+      e.as = r[(kRecE + 5) * 32];
+      e.b1 = r[(kRecE + 6) * 32];
+      e.b2 = r[(kRecE + 7) * 32];
+      e.sbn = r[(kRecE + 8) * 32];
+      e.vn = r[(kRecE + 9) * 32];
+      e.vt1 = r[(kRecE + 10) * 32];
+      e.vt2 = r[(kRecE + 11) * 32];
+      e.ia2 = r[(kRecE + 12) * 32];
+      e.ra2 = r[(kRecE + 13) * 32];
+      e.hv2 = r[(kRecE + 14) * 32];
+      e.ir = r[(kRecE + 15) * 32];
+      e.isr = r[(kRecE + 16) * 32];
+      e.gm1 = gm1;
+      e.igm = igm;
+      double Ra[7], Rb[7];
+      wave_lr(e, ka, La, Ra);
+      wave_lr(e, kb, Lb, Rb);
+#pragma unroll
+      for (int m = 0; m < 7; ++m) grp[kGrpR + ka * 7 + m] = Ra[m];
+      if (two) {
+#pragma unroll
+        for (int m = 0; m < 7; ++m) grp[kGrpR + kb * 7 + m] = Rb[m];
+      }
+    }
+    __syncwarp();
+    // L R = I within 1024 ulp (mhd_eigensystem.hpp:416-430): this lane's L
+    // rows against every R column; |d| <= 1024 eps tested as
+    // d^2 <= (1024 eps)^2
+    if (on) {
+#pragma unroll
+      for (int jc = 0; jc < 7; ++jc) {
+        double R7[7];
+#pragma unroll
+        for (int m = 0; m < 7; ++m) R7[m] = grp[kGrpR + jc * 7 + m];
+        double da = 0.0, db = 0.0;
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+          da += La[m] * R7[m];
+          db += Lb[m] * R7[m];
+        }
+        const double ea = da - (ka == jc ? 1.0 : 0.0), eb = db - (kb == jc ? 1.0 : 0.0);
+        ok = ok && (ea * ea <= kT2) && (eb * eb <= kT2);
+      }
+    }
+    const unsigned okm = __ballot_sync(0xffffffffu, ok);
+    const bool usable = ((okm >> (gi * 4)) & 0xFu) == 0xFu;
+    if (on && !usable) {
+#pragma unroll
+      for (int v = 0; v < 7; ++v) {
+        La[v] = v == ka ? 1.0 : 0.0;
+        Lb[v] = v == kb ? 1.0 : 0.0;
+        grp[kGrpR + ka * 7 + v] = v == ka ? 1.0 : 0.0;
+        if (two) grp[kGrpR + kb * 7 + v] = v == kb ? 1.0 : 0.0;
+      }
+    }
+    // stencil deltas in the canonical frame: lane rl loads cells rl, rl + 4
+    if (on) {
+      const double* r = rec + f;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int sc = rl + 4 * h;
+        if (sc < S) {
+          const St d = rot<DIR>(load_cell(u, kf + (long long)(sc - 1 - H) * step));
+          double* dd = grp + kGrpD + sc * 7;
+          dd[0] = d.rho - r[(kRecC + 0) * 32];
+          dd[1] = d.mx - r[(kRecC + 1) * 32];
+          dd[2] = d.my - r[(kRecC + 2) * 32];
+          dd[3] = d.mz - r[(kRecC + 3) * 32];
+          dd[4] = d.E - r[(kRecC + 4) * 32];
+          dd[5] = d.by - r[(kRecC + 6) * 32];
+          dd[6] = d.bz - r[(kRecC + 7) * 32];
+        }
+      }
+    }
+    __syncwarp();
+    // projection onto this lane's waves
+    double cha[S], chb[S];
+    if (on) {
+#pragma unroll
+      for (int sc = 0; sc < S; ++sc) {
+        double d7[7];
+#pragma unroll
+        for (int v = 0; v < 7; ++v) d7[v] = grp[kGrpD + sc * 7 + v];
+        double aa = 0.0, ab = 0.0;
+#pragma unroll
+        for (int v = 0; v < 7; ++v) {
+          aa += La[v] * d7[v];
+          ab += Lb[v] * d7[v];
+        }
+        cha[sc] = aa;
+        chb[sc] = ab;
+      }
+    }
+    __syncwarp();  // the deltas are read; w overwrites them
+    // MP limiter on both sides of both waves
+    if (on) {
+      double win[W];
+      bool fl;
+#pragma unroll
+      for (int sc = 0; sc < W; ++sc) win[sc] = cha[sc];
+      grp[kGrpW + ka] = mp_recon<W>(win, fl);
+#pragma unroll
+      for (int sc = 0; sc < W; ++sc) win[sc] = cha[W - sc];
+      grp[kGrpW + 7 + ka] = mp_recon<W>(win, fl);
+      if (two) {
+#pragma unroll
+        for (int sc = 0; sc < W; ++sc) win[sc] = chb[sc];
+        grp[kGrpW + kb] = mp_recon<W>(win, fl);
+#pragma unroll
+        for (int sc = 0; sc < W; ++sc) win[sc] = chb[W - sc];
+        grp[kGrpW + 7 + kb] = mp_recon<W>(win, fl);
+      }
+    }
+    __syncwarp();
+    // back-projection: lane rl forms components rl and rl + 4 of both sides
+    if (on) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int v = rl + 4 * h;
+        if (v < 7) {
+          double dl = 0.0, dr = 0.0;
+#pragma unroll
+          for (int q = 0; q < 7; ++q) {
+            const double rq = grp[kGrpR + q * 7 + v];
+            dl += rq * grp[kGrpW + q];
+            dr += rq * grp[kGrpW + 7 + q];
+          }
+          rec[(kRecE + v) * 32 + f] = dl;
+          rec[(kRecE + 7 + v) * 32 + f] = dr;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // phase 3: this lane's face
+  if (!valid) return;
+  const double* r = rec + lane;
+  St c;
+  c.rho = r[(kRecC + 0) * 32];
+  c.mx = r[(kRecC + 1) * 32];
+  c.my = r[(kRecC + 2) * 32];
+  c.mz = r[(kRecC + 3) * 32];
+  c.E = r[(kRecC + 4) * 32];
+  c.bx = r[(kRecC + 5) * 32];
+  c.by = r[(kRecC + 6) * 32];
+  c.bz = r[(kRecC + 7) * 32];
+  double dl[7], dr[7];
+#pragma unroll
+  for (int v = 0; v < 7; ++v) {
+    dl[v] = r[(kRecE + v) * 32];
+    dr[v] = r[(kRecE + 7 + v) * 32];
+  }
+  const St sl{c.rho + dl[0], c.mx + dl[1], c.my + dl[2], c.mz + dl[3],
+              c.E + dl[4],   c.bx,         c.by + dl[5], c.bz + dl[6]};
+  const St sr{c.rho + dr[0], c.mx + dr[1], c.my + dr[2], c.mz + dr[3],
+              c.E + dr[4],   c.bx,         c.by + dr[5], c.bz + dr[6]};
+  finish_face<DIR, ORDER, 0>(g, u, out, gamma, i, j, k0, step, rot<DIR>(sl), rot<DIR>(sr));
+}
+
 // ---- MUSCL-minmod in primitive variables (mhd_reconstruct.hip:93-404) ----
 __device__ __forceinline__ int slope_drop(int c, int n, int lo, int hi) {
   if (lo != 0 && lo != 4 && c <= 0) return -1;
@@ -805,10 +1124,21 @@ __device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const
         atomicMax(label + k0, __float_as_int(limiter_departure(ur, lr)));
       }
     }
-    if constexpr (MODE != 2) {
-      if (!recon_admissible(ul, gamma) || !recon_admissible(ur, gamma))
-        muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
-    }
+  }
+  finish_face<DIR, ORDER, MODE>(g, u, out, gamma, i, j, k0, step, ul, ur);
+}
+
+// The fallback chain after the high-order states of one face
+// (mhd_reconstruct.hip:514-670): MUSCL when a characteristic MP state is not
+// admissible, the shared CT normal field, first order, then NaN; the states
+// are written to the face's interface slots.
+template <int DIR, int ORDER, int MODE>
+__device__ __forceinline__ void finish_face(const Grid& g, const StateP& u, const IfaceP& out,
+                                            double gamma, int i, int j, long long k0,
+                                            long long step, St ul, St ur) {
+  if constexpr (ORDER >= 5 && MODE != 2) {
+    if (!recon_admissible(ul, gamma) || !recon_admissible(ur, gamma))
+      muscl_pair<DIR>(g, u, i, j, k0, step, gamma, ul, ur);
   }
   const double bn = (DIR == 0 ? u.c[5] : u.c[6])[k0];
   set_normal_b<DIR>(ul, bn);
@@ -844,14 +1174,21 @@ __device__ __forceinline__ void b_reconstruct(const Grid& g, const StateP& u, co
   // dir 0: faces i in [0,nx] over all padded rows; dir 1: transposed.
   const int i = bx * blockDim.x + threadIdx.x - (DIR == 1 ? g.ng : 0);
   const int j = by * blockDim.y + threadIdx.y - (DIR == 0 ? g.ng : 0);
-  if (DIR == 0 ? (i > g.nx || j >= g.ny + g.ng) : (i >= g.nx + g.ng || j > g.ny)) return;
-  if (ctl->status & ~kStatusDone) return;
+  const bool valid = !(DIR == 0 ? (i > g.nx || j >= g.ny + g.ng) : (i >= g.nx + g.ng || j > g.ny));
+  if (ctl->status & ~kStatusDone) return;  // uniform: no kernel of a step writes it mid-launch
+  if constexpr (MODE == 0 && ORDER >= 5) {
+    // the characteristic path, warp-cooperative (threadIdx.y = warp)
+    extern __shared__ double dsm[];
+    mp_faces_warp<DIR, ORDER>(g, u, out, gamma, i, j, valid, dsm + threadIdx.y * kWarpReconDoubles);
+    return;
+  }
+  if (!valid) return;
   recon_face<DIR, ORDER, MODE>(g, u, out, gamma, i, j, label, defer);
 }
 
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128) k_reconstruct(Grid g, StateP u, IfaceP out, double gamma,
-                                                     const Ctl* ctl) {
+__global__ void __launch_bounds__(128, 4) k_reconstruct(Grid g, StateP u, IfaceP out, double gamma,
+                                                        const Ctl* ctl) {
   b_reconstruct<DIR, ORDER>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y);
 }
 
@@ -874,17 +1211,34 @@ __global__ void __launch_bounds__(128, 5) k_reconstruct_lin(Grid g, StateP u, If
 
 // Learned mode, pass 2: the listed faces (padded linear index of the face's
 // high cell) by the full characteristic path; the count is read on the device.
+// Warps take 32 consecutive list entries at a time.
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128) k_reconstruct_list(Grid g, StateP u, IfaceP out,
-                                                          double gamma, const Ctl* ctl,
-                                                          const int* list, const int* count) {
-  if (ctl->status & ~kStatusDone) return;
-  const int n = *count;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int k = list[t];
-    const int i = k % g.pitch - g.ng, j = k / g.pitch - g.ng;
-    recon_face<DIR, ORDER, 0>(g, u, out, gamma, i, j, nullptr);
+__device__ __forceinline__ void b_reconstruct_list(const Grid& g, const StateP& u,
+                                                   const IfaceP& out, double gamma,
+                                                   const int* list, int n) {
+  extern __shared__ double dsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* ws = dsm + warp * kWarpReconDoubles;
+  for (int base = (blockIdx.x * kReconWarps + warp) * 32; base < n;
+       base += gridDim.x * kReconWarps * 32) {
+    const int t = base + lane;
+    const bool valid = t < n;
+    int i = 0, j = 0;
+    if (valid) {
+      const int k = list[t];
+      i = k % g.pitch - g.ng;
+      j = k / g.pitch - g.ng;
+    }
+    mp_faces_warp<DIR, ORDER>(g, u, out, gamma, i, j, valid, ws);
   }
+}
+
+template <int DIR, int ORDER>
+__global__ void __launch_bounds__(128, 4) k_reconstruct_list(Grid g, StateP u, IfaceP out,
+                                                             double gamma, const Ctl* ctl,
+                                                             const int* list, const int* count) {
+  if (ctl->status & ~kStatusDone) return;
+  b_reconstruct_list<DIR, ORDER>(g, u, out, gamma, list, *count);
 }
 
 // Faces whose either cell is flagged, appended to the x and y lists in
@@ -1863,7 +2217,7 @@ __global__ void k_cell_sums(Grid g, StateP u, double* partial) {
 namespace {
 
 template <int DIR, int ORDER, int MODE = 0>
-__global__ void __launch_bounds__(128) kb_reconstruct(const BatchRec* __restrict__ r, BatchPlan p,
+__global__ void __launch_bounds__(128, 4) kb_reconstruct(const BatchRec* __restrict__ r, BatchPlan p,
                                                       const BatchLearnRec* __restrict__ l = nullptr) {
   for (int t = blockIdx.x; t < p.total; t += gridDim.x) {
     int local, bx, by;
@@ -1882,20 +2236,14 @@ __global__ void __launch_bounds__(128) kb_reconstruct(const BatchRec* __restrict
 // Characteristic pass over every instance's face list: each CTA takes its
 // share of each instance's list in turn.
 template <int DIR, int ORDER>
-__global__ void __launch_bounds__(128) kb_reconstruct_list(const BatchRec* __restrict__ r,
-                                                           const BatchLearnRec* __restrict__ l,
-                                                           int n) {
+__global__ void __launch_bounds__(128, 4) kb_reconstruct_list(const BatchRec* __restrict__ r,
+                                                              const BatchLearnRec* __restrict__ l,
+                                                              int n) {
   for (int inst = 0; inst < n; ++inst) {
     const BatchRec& q = r[inst];
     if (q.a.ctl->status & ~kStatusDone) continue;
-    const int cnt = l[inst].counts[DIR];
-    const int* list = DIR == 0 ? l[inst].xlist : l[inst].ylist;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-      const int k = list[t];
-      const int i = k % q.a.g.pitch - q.a.g.ng, j = k / q.a.g.pitch - q.a.g.ng;
-      recon_face<DIR, ORDER, 0>(q.a.g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma, i, j,
-                                nullptr);
-    }
+    b_reconstruct_list<DIR, ORDER>(q.a.g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma,
+                                   DIR == 0 ? l[inst].xlist : l[inst].ylist, l[inst].counts[DIR]);
   }
 }
 
@@ -2084,7 +2432,7 @@ static void recon_launch(const StageArgs& a, cudaStream_t s) {
   const dim3 grid(cdiv(ni, kBX), cdiv(nj, 4));
   size_t smem = 0;
   if (ORDER == 5 || ORDER == 7) {
-    smem = kReconSmem;
+    smem = kReconWarpSmem;
     ensure_smem((const void*)k_reconstruct<DIR, ORDER>, smem);
   }
   k_reconstruct<DIR, ORDER><<<grid, block, smem, s>>>(g, a.u, DIR == 0 ? a.ix : a.iy, a.gamma,
@@ -2232,15 +2580,15 @@ int batch_phase_max_ctas_per_sm(int phase, int order) {
   const bool o7 = order == 7;
   switch (phase) {
     case kBpRecon0:
-      ensure_smem((const void*)kb_reconstruct<0, 7>, kReconSmem);
-      ensure_smem((const void*)kb_reconstruct<0, 5>, kReconSmem);
-      return o7 ? max_ctas(kb_reconstruct<0, 7>, 128, kReconSmem)
-                : max_ctas(kb_reconstruct<0, 5>, 128, kReconSmem);
+      ensure_smem((const void*)kb_reconstruct<0, 7>, kReconWarpSmem);
+      ensure_smem((const void*)kb_reconstruct<0, 5>, kReconWarpSmem);
+      return o7 ? max_ctas(kb_reconstruct<0, 7>, 128, kReconWarpSmem)
+                : max_ctas(kb_reconstruct<0, 5>, 128, kReconWarpSmem);
     case kBpRecon1:
-      ensure_smem((const void*)kb_reconstruct<1, 7>, kReconSmem);
-      ensure_smem((const void*)kb_reconstruct<1, 5>, kReconSmem);
-      return o7 ? max_ctas(kb_reconstruct<1, 7>, 128, kReconSmem)
-                : max_ctas(kb_reconstruct<1, 5>, 128, kReconSmem);
+      ensure_smem((const void*)kb_reconstruct<1, 7>, kReconWarpSmem);
+      ensure_smem((const void*)kb_reconstruct<1, 5>, kReconWarpSmem);
+      return o7 ? max_ctas(kb_reconstruct<1, 7>, 128, kReconWarpSmem)
+                : max_ctas(kb_reconstruct<1, 5>, 128, kReconWarpSmem);
     case kBpFlux: {
       constexpr int t = kFqThreads;
       return o7 ? max_ctas(kb_face_flux_q<0, 7>, t, 0) : max_ctas(kb_face_flux_q<0, 5>, t, 0);
@@ -2264,19 +2612,19 @@ void launch_batch_reconstruct(const BatchRec* r, const BatchPlan& p, int dir, in
   const dim3 block(32, 4);
   if (order == 7) {
     if (dir == 0) {
-      ensure_smem((const void*)kb_reconstruct<0, 7>, kReconSmem);
-      kb_reconstruct<0, 7><<<pgrid(p), block, kReconSmem, s>>>(r, p);
+      ensure_smem((const void*)kb_reconstruct<0, 7>, kReconWarpSmem);
+      kb_reconstruct<0, 7><<<pgrid(p), block, kReconWarpSmem, s>>>(r, p);
     } else {
-      ensure_smem((const void*)kb_reconstruct<1, 7>, kReconSmem);
-      kb_reconstruct<1, 7><<<pgrid(p), block, kReconSmem, s>>>(r, p);
+      ensure_smem((const void*)kb_reconstruct<1, 7>, kReconWarpSmem);
+      kb_reconstruct<1, 7><<<pgrid(p), block, kReconWarpSmem, s>>>(r, p);
     }
   } else {
     if (dir == 0) {
-      ensure_smem((const void*)kb_reconstruct<0, 5>, kReconSmem);
-      kb_reconstruct<0, 5><<<pgrid(p), block, kReconSmem, s>>>(r, p);
+      ensure_smem((const void*)kb_reconstruct<0, 5>, kReconWarpSmem);
+      kb_reconstruct<0, 5><<<pgrid(p), block, kReconWarpSmem, s>>>(r, p);
     } else {
-      ensure_smem((const void*)kb_reconstruct<1, 5>, kReconSmem);
-      kb_reconstruct<1, 5><<<pgrid(p), block, kReconSmem, s>>>(r, p);
+      ensure_smem((const void*)kb_reconstruct<1, 5>, kReconWarpSmem);
+      kb_reconstruct<1, 5><<<pgrid(p), block, kReconWarpSmem, s>>>(r, p);
     }
   }
 }
@@ -2345,22 +2693,22 @@ void launch_batch_reconstruct_learned(const BatchRec* r, const BatchLearnRec* l,
   if (order == 7) {
     if (dir == 0) {
       kb_reconstruct<0, 7, 2><<<pgrid(p), block, 0, s>>>(r, p, l);
-      ensure_smem((const void*)kb_reconstruct_list<0, 7>, kReconSmem);
-      kb_reconstruct_list<0, 7><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
+      ensure_smem((const void*)kb_reconstruct_list<0, 7>, kReconWarpSmem);
+      kb_reconstruct_list<0, 7><<<list_grid, 128, kReconWarpSmem, s>>>(r, l, p.n);
     } else {
       kb_reconstruct<1, 7, 2><<<pgrid(p), block, 0, s>>>(r, p, l);
-      ensure_smem((const void*)kb_reconstruct_list<1, 7>, kReconSmem);
-      kb_reconstruct_list<1, 7><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
+      ensure_smem((const void*)kb_reconstruct_list<1, 7>, kReconWarpSmem);
+      kb_reconstruct_list<1, 7><<<list_grid, 128, kReconWarpSmem, s>>>(r, l, p.n);
     }
   } else {
     if (dir == 0) {
       kb_reconstruct<0, 5, 2><<<pgrid(p), block, 0, s>>>(r, p, l);
-      ensure_smem((const void*)kb_reconstruct_list<0, 5>, kReconSmem);
-      kb_reconstruct_list<0, 5><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
+      ensure_smem((const void*)kb_reconstruct_list<0, 5>, kReconWarpSmem);
+      kb_reconstruct_list<0, 5><<<list_grid, 128, kReconWarpSmem, s>>>(r, l, p.n);
     } else {
       kb_reconstruct<1, 5, 2><<<pgrid(p), block, 0, s>>>(r, p, l);
-      ensure_smem((const void*)kb_reconstruct_list<1, 5>, kReconSmem);
-      kb_reconstruct_list<1, 5><<<list_grid, 128, kReconSmem, s>>>(r, l, p.n);
+      ensure_smem((const void*)kb_reconstruct_list<1, 5>, kReconWarpSmem);
+      kb_reconstruct_list<1, 5><<<list_grid, 128, kReconWarpSmem, s>>>(r, l, p.n);
     }
   }
 }
@@ -2400,8 +2748,8 @@ void launch_reconstruct_learned(const StageArgs& a, int dir, const unsigned char
   if (dir == D && a.order == O) {                                                              \
     k_reconstruct_lin<D, O><<<recon_grid<D, O>(a.g), block, 0, s>>>(a.g, a.u, out, a.gamma,    \
                                                                     a.ctl, defer);             \
-    ensure_smem((const void*)k_reconstruct_list<D, O>, kReconSmem);                             \
-    k_reconstruct_list<D, O><<<list_grid, 128, kReconSmem, s>>>(a.g, a.u, out, a.gamma, a.ctl,   \
+    ensure_smem((const void*)k_reconstruct_list<D, O>, kReconWarpSmem);                         \
+    k_reconstruct_list<D, O><<<list_grid, 128, kReconWarpSmem, s>>>(a.g, a.u, out, a.gamma, a.ctl,   \
                                                                 list, count);                  \
     return;                                                                                    \
   }
