@@ -1761,13 +1761,19 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
   if (s_stop) return;
   const int i0 = bx * TX, j0 = by * TY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-#pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const double* src = c < 5 ? u.c[c] : c == 5 ? u.bxc : c == 6 ? u.byc : u.c[7];
-    for (int e = tid; e < SY * SX; e += TX * TY) {
-      const int r = e / SX, x = e - r * SX;
+  // staging: one index computation per staged cell, its 8 components
+  // loaded with the same offset
+  for (int r = threadIdx.y; r < SY; r += TY) {
+    for (int x = threadIdx.x; x < SX; x += TX) {
       const int ii = i0 - H + x, jj = j0 - H + r;
-      S[c * SY * SX + e] = in_pad(g, ii, jj) ? __ldg(src + g.idx(ii, jj)) : 0.0;
+      const bool in = in_pad(g, ii, jj);
+      const long long kk = in ? g.idx(ii, jj) : 0;
+      double* dst = S + r * SX + x;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const double* src = c < 5 ? u.c[c] : c == 5 ? u.bxc : c == 6 ? u.byc : u.c[7];
+        dst[c * SY * SX] = in ? __ldg(src + kk) : 0.0;
+      }
     }
   }
   __syncthreads();
@@ -1781,14 +1787,17 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
     double wx[N];
 #pragma unroll
     for (int t = 0; t < N; ++t) wx[t] = point_w<ORDER>(qx, t);
-    for (int e = tid; e < 8 * SY * TX; e += TX * TY) {
-      const int c = e / (SY * TX), rem = e - c * SY * TX;
-      const int r = rem / TX, x = rem - r * TX;
-      const double* row = S + (c * SY + r) * SX + x;
+    // x-recovery of every staged row (component c, row r) at this x node:
+    // row task t = c * SY + r, TY of them at a time, lane = column
+    static_assert((8 * SY) % TY == 0, "row tasks divide evenly over the block's rows");
+#pragma unroll
+    for (int m = 0; m < 8 * SY / TY; ++m) {
+      const int t = threadIdx.y + m * TY;
+      const double* row = S + t * SX + threadIdx.x;
       double smp[N];
 #pragma unroll
-      for (int t = 0; t < N; ++t) smp[t] = row[t];
-      X[e] = wsum<N>(wx, smp);
+      for (int q = 0; q < N; ++q) smp[q] = row[q];
+      X[t * TX + threadIdx.x] = wsum<N>(wx, smp);
     }
     __syncthreads();
     if (active && ok) {
