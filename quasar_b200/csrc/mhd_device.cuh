@@ -71,6 +71,23 @@ __device__ __forceinline__ double exact_dot(const double* w, const double* x) {
   return __dadd_rn(s, c);
 }
 
+// ---- division by a cell size ----------------------------------------------
+// Reciprocal of h when h is a power of two whose reciprocal is a normal
+// number (then it is exact), else 0.
+__device__ __forceinline__ double pow2_recip(double h) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(h);
+  const unsigned e = unsigned(b >> 52) & 0x7ffu;
+  const bool pow2 = (b & 0x000fffffffffffffull) == 0ull && e >= 2u && e <= 2044u;
+  return pow2 ? 1.0 / h : 0.0;
+}
+// x / h, formed as x * (1/h) where pow2_recip gave the exact reciprocal rh:
+// both are the correctly rounded value of the same real number, so the bits
+// are those of the division (every grid whose side is a power-of-two number
+// of cells on a unit box takes the multiplication).
+__device__ __forceinline__ double div_by(double x, double h, double rh) {
+  return rh != 0.0 ? __dmul_rn(x, rh) : __ddiv_rn(x, h);
+}
+
 // ---- EOS helpers: numerics/mhd_state.hpp ---------------------------------
 // Evaluated without FMA contraction, in the reference's operation order: at a
 // degenerate wave fan (zero transverse field) the eigenvector weights are

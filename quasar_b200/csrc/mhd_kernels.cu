@@ -66,7 +66,7 @@ __device__ __forceinline__ double low_order_b(const double* f, const Grid& g, in
                                               int hi, long long k, long long step) {
   const double lo_face = f[k];
   if (cell >= hi) return lo_face;
-  return __ddiv_rn(__dadd_rn(lo_face, f[k + step]), 2.0);
+  return __dmul_rn(__dadd_rn(lo_face, f[k + step]), 0.5);  // = / 2 exactly
 }
 __device__ __forceinline__ St load_cell1(const StateP& u, const Grid& g, int i, int j) {
   const long long k = g.idx(i, j);
@@ -284,12 +284,13 @@ __device__ __forceinline__ void divb_cell(const Grid& g, const StateP& u, long l
                                           unsigned long long& sb) {
   const double bxl = u.c[5][k], bxh = u.c[5][k + 1];
   const double byl = u.c[6][k], byh = u.c[6][k + g.pitch];
-  const double d1 = __ddiv_rn(__dadd_rn(bxh, -bxl), g.dx);
-  const double d2 = __ddiv_rn(__dadd_rn(byh, -byl), g.dy);
+  const double rdx = pow2_recip(g.dx), rdy = pow2_recip(g.dy);
+  const double d1 = div_by(__dadd_rn(bxh, -bxl), g.dx, rdx);
+  const double d2 = div_by(__dadd_rn(byh, -byl), g.dy, rdy);
   const double res = __dadd_rn(d1, d2);
   const double scale = __dadd_rn(fabs(d1), fabs(d2));
-  const double unc = __dadd_rn(__ddiv_rn(__dadd_rn(ulp_of(bxh), ulp_of(bxl)), g.dx),
-                               __ddiv_rn(__dadd_rn(ulp_of(byh), ulp_of(byl)), g.dy));
+  const double unc = __dadd_rn(div_by(__dadd_rn(ulp_of(bxh), ulp_of(bxl)), g.dx, rdx),
+                               div_by(__dadd_rn(ulp_of(byh), ulp_of(byl)), g.dy, rdy));
   bool explained;
   if (solver_owned) {
     explained = fabs(res) <= 1024.0 * unc;
@@ -1315,7 +1316,7 @@ __device__ __forceinline__ double face_rate(const St& l, const St& r, double gam
   const Spd a = speed_parts<DIR>(l, gamma), b = speed_parts<DIR>(r, gamma);
   const double rate = ORDER <= 1 ? fmax(a.v + a.f, b.v + b.f) : fmax(a.v, b.v) + fmax(a.f, b.f);
   if (!(isfinite(rate) && rate >= 0.0)) return kInf;
-  return (rate * 0.5) / h;
+  return div_by(rate * 0.5, h, pow2_recip(h));
 }
 
 __device__ __forceinline__ St iface(const IfaceP& v, long long k, bool left) {
@@ -1864,7 +1865,7 @@ __device__ __forceinline__ double edge_interp(const double* e) {
 #pragma unroll
   for (int q = 1; q < NT; ++q) same = same && (e[q] == e[0]);
   if (same) return e[0];
-  if (NT == 2) return __ddiv_rn(__dadd_rn(e[0], e[1]), 2.0);
+  if (NT == 2) return __dmul_rn(__dadd_rn(e[0], e[1]), 0.5);  // = / 2 exactly
   if (NT == 6)
     return (((((e[0] - 8.0 * e[1]) + 37.0 * e[2]) + 37.0 * e[3]) - 8.0 * e[4]) + e[5]) / 60.0;
   return (((((((-3.0 * e[0] + 29.0 * e[1]) - 139.0 * e[2]) + 533.0 * e[3]) + 533.0 * e[4]) -
@@ -2068,24 +2069,26 @@ __device__ __forceinline__ void b_update(const Grid& g, const StateP& un, const 
     return crsum3(__dmul_rn(a, vn), __dmul_rn(b, vs), __dmul_rn(c, d));
   };
   const long long k = g.idx(i, j);
+  const double rdx = pow2_recip(g.dx), rdy = pow2_recip(g.dy);
   if (i < g.nx && j < g.ny) {
     const int cc[6] = {0, 1, 2, 3, 4, 7};
 #pragma unroll
     for (int t = 0; t < 6; ++t) {
       const int q = cc[t];
-      const double dqx = __dadd_rn(__ddiv_rn(fx.f[q][k + 1], g.dx), __ddiv_rn(-fx.f[q][k], g.dx));
+      const double dqx =
+          __dadd_rn(div_by(fx.f[q][k + 1], g.dx, rdx), div_by(-fx.f[q][k], g.dx, rdx));
       const double dqy =
-          __dadd_rn(__ddiv_rn(fy.f[q][k + g.pitch], g.dy), __ddiv_rn(-fy.f[q][k], g.dy));
+          __dadd_rn(div_by(fy.f[q][k + g.pitch], g.dy, rdy), div_by(-fy.f[q][k], g.dy, rdy));
       const double d = __dadd_rn(-dqx, -dqy);
       out.c[q][k] = combine(un.c[q][k], b == 0.0 ? 0.0 : us.c[q][k], d);
     }
   }
   if (j < g.ny) {
-    const double d = __dadd_rn(__ddiv_rn(-ez[k + g.pitch], g.dy), __ddiv_rn(ez[k], g.dy));
+    const double d = __dadd_rn(div_by(-ez[k + g.pitch], g.dy, rdy), div_by(ez[k], g.dy, rdy));
     out.c[5][k] = combine(un.c[5][k], b == 0.0 ? 0.0 : us.c[5][k], d);
   }
   if (i < g.nx) {
-    const double d = __dadd_rn(__ddiv_rn(ez[k + 1], g.dx), __ddiv_rn(-ez[k], g.dx));
+    const double d = __dadd_rn(div_by(ez[k + 1], g.dx, rdx), div_by(-ez[k], g.dx, rdx));
     out.c[6][k] = combine(un.c[6][k], b == 0.0 ? 0.0 : us.c[6][k], d);
   }
 }
@@ -2175,9 +2178,10 @@ __global__ void k_divb_linf(Grid g, StateP u, unsigned long long* out) {
   if (i >= g.nx || j >= g.ny) return;
   const long long k = g.idx(i, j);
   // ct_divb_linf_kernel (mhd_reduce.hip:505-553)
-  const double d = __dadd_rn(__dadd_rn(__ddiv_rn(u.c[5][k + 1], g.dx), __ddiv_rn(-u.c[5][k], g.dx)),
-                             __dadd_rn(__ddiv_rn(u.c[6][k + g.pitch], g.dy),
-                                       __ddiv_rn(-u.c[6][k], g.dy)));
+  const double rdx = pow2_recip(g.dx), rdy = pow2_recip(g.dy);
+  const double d = __dadd_rn(__dadd_rn(div_by(u.c[5][k + 1], g.dx, rdx), div_by(-u.c[5][k], g.dx, rdx)),
+                             __dadd_rn(div_by(u.c[6][k + g.pitch], g.dy, rdy),
+                                       div_by(-u.c[6][k], g.dy, rdy)));
   const double v = isfinite(d) ? fabs(d) : kInf;
   atomic_max_lanes(out, v > 0.0 ? dbits(v) : 0ull);
 }
@@ -2792,10 +2796,10 @@ __global__ void __launch_bounds__(256) k_abi_flux_difference(Grid g, FluxP f, in
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= g.nx || j >= g.ny) return;
   const long long k = g.idx(i, j), kp = k + (dir == 0 ? 1 : g.pitch);
-  const double h = dir == 0 ? g.dx : g.dy;
+  const double h = dir == 0 ? g.dx : g.dy, rh = pow2_recip(h);
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
-    const double dq = __dadd_rn(__ddiv_rn(f.f[q][kp], h), __ddiv_rn(-f.f[q][k], h));
+    const double dq = __dadd_rn(div_by(f.f[q][kp], h, rh), div_by(-f.f[q][k], h, rh));
     d.f[q][k] = __dadd_rn(d.f[q][k], -dq);
   }
 }
@@ -2808,8 +2812,9 @@ __global__ void __launch_bounds__(256) k_abi_curl_rate(Grid g, const double* __r
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i > g.nx || j > g.ny) return;
   const long long k = g.idx(i, j);
-  if (j < g.ny) dbx[k] = __dadd_rn(__ddiv_rn(-ez[k + g.pitch], g.dy), __ddiv_rn(ez[k], g.dy));
-  if (i < g.nx) dby[k] = __dadd_rn(__ddiv_rn(ez[k + 1], g.dx), __ddiv_rn(-ez[k], g.dx));
+  const double rdx = pow2_recip(g.dx), rdy = pow2_recip(g.dy);
+  if (j < g.ny) dbx[k] = __dadd_rn(div_by(-ez[k + g.pitch], g.dy, rdy), div_by(ez[k], g.dy, rdy));
+  if (i < g.nx) dby[k] = __dadd_rn(div_by(ez[k + 1], g.dx, rdx), div_by(-ez[k], g.dx, rdx));
 }
 
 // out = a un + b us + c dudt (mhd_update.hip:113-206): an operand whose weight
