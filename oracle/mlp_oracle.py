@@ -1,7 +1,8 @@
 """CPU restatement of the troubled-cell indicator network (test infrastructure:
 only tests import it; the product path never does).
 
-200 -> 64 -> 64 -> 1 with exact-erf GELU.  The GPU kernels multiply BF16
+200 -> 64 -> 64 -> 1 with the tanh-form GELU (exact tanh here; the kernels
+use the hardware tanh approximation).  The GPU kernels multiply BF16
 operands (features, w1, w2 and the first hidden activation) with FP32
 accumulation; `bf16` rounds to nearest even so this restatement sees the
 same operands, then computes in float64.  Parity is therefore to FP32
@@ -10,7 +11,6 @@ accumulation order, not bit for bit.
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 FEAT, HID = 200, 64
 NPARAM = HID * FEAT + HID + HID * HID + HID + HID + 1
@@ -35,12 +35,17 @@ def unpack(p):
     return w1, b1, w2, b2, w3, b3
 
 
+K0, K1 = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    """tanh-form GELU (Hendrycks and Gimpel), the activation the kernels use."""
+    return 0.5 * x * (1.0 + np.tanh(K0 * (x + K1 * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(K0 * (x + K1 * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * K0 * (1.0 + 3.0 * K1 * x * x)
 
 
 def forward(params, X):

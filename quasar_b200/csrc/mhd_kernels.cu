@@ -2744,10 +2744,11 @@ void launch_reconstruct_label(const StageArgs& a, int dir, int* label, cudaStrea
   const dim3 block(kBX, 4);
   const IfaceP out = dir == 0 ? a.ix : a.iy;
 #define QB_LBL(D, O)                                                                          \
-  if (dir == D && a.order == O)                                                              \
+  if (dir == D && a.order == O) {                                                            \
     ensure_smem((const void*)k_reconstruct_label<D, O>, kReconSmem);                          \
     return (void)k_reconstruct_label<D, O><<<recon_grid<D, O>(a.g), block, kReconSmem, s>>>( \
-        a.g, a.u, out, a.gamma, a.ctl, label);
+        a.g, a.u, out, a.gamma, a.ctl, label);                                                \
+  }
   QB_LBL(0, 5) QB_LBL(1, 5) QB_LBL(0, 7) QB_LBL(1, 7)
 #undef QB_LBL
 }

@@ -60,14 +60,14 @@ def main(argv=None):
     ap.add_argument("--runs", type=int, default=12)
     ap.add_argument("--snapshots", type=int, default=20)
     ap.add_argument("--order", type=int, default=5)
-    ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--tiles", type=int, default=512)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--pos-weight", type=float, default=30.0)
-    ap.add_argument("--recall", type=float, default=0.99)
+    ap.add_argument("--recall", type=float, default=0.95)
     ap.add_argument("--holdout", type=int, default=20)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--tol", type=float, default=1e-5)
+    ap.add_argument("--tol", type=float, default=1e-4)
     a = ap.parse_args(argv)
     a.out = a.out or default_path(a.order)
     ind = TroubledCellIndicator(seed=a.seed)

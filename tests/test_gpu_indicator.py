@@ -137,3 +137,45 @@ def test_inference_report_on_developed_orszag_tang():
     # round-off level (both are random walks of the same rounding statistics)
     assert r["div_b_rel"] < 1e-11, r
     assert r["div_b_rel"] <= 2.0 * max(r["div_b_rel_plain"], 1e-15), r
+
+
+def _tube(n, order, axis):
+    """A Brio-Wu-like tube varying along one axis only (outflow): the normal
+    field uniform, the tangential field and the gas jumping at the middle."""
+    from quasar_b200 import ics, mhd
+    ng = ics.nghost(order)
+    X, Y = np.meshgrid(ics._centres(n, ng, 1.0, 0.0), ics._centres(n, ng, 1.0, 0.0), indexing="xy")
+    s = X if axis == 0 else Y
+    left = s < 0.5
+    rho, p = np.where(left, 1.0, 0.125), np.where(left, 1.0, 0.1)
+    bt = np.where(left, 1.0, -1.0)
+    zero = np.zeros_like(X)
+    bx, by = (zero + 0.75, bt) if axis == 0 else (bt, zero + 0.75)
+    comps = ics._assemble(rho, zero, zero, zero, p, bx, by, zero, 2.0)
+    cfg = mhd.MhdConfig()
+    cfg.grid = mhd.Grid2D(n, n, 1.0, 1.0)
+    cfg.reconstruction = "mp5" if order == 5 else "mp7"
+    cfg.gamma = 2.0
+    cfg.boundary = mhd.MhdBoundarySpec(["outflow"] * 4, ["outflow"] * 4)
+    sv = mhd.MhdSolver2D(cfg)
+    for name, a in zip(ics.COMPONENTS, comps):
+        sv.seed_state(name, a)
+    return sv
+
+
+@pytest.mark.parametrize("order", [5, 7])
+def test_labels_come_from_both_face_directions(order):
+    """Limiter labels of a tube along x and of the same tube along y: only the
+    faces normal to the tube see its jump, so the labels of one come from x
+    faces and of the other from y faces alone; by symmetry their counts agree,
+    and both orders collect."""
+    from quasar_b200.indicator import TroubledCellIndicator
+    counts = []
+    for axis in (0, 1):
+        s = _tube(64, order, axis)
+        for _ in range(4):
+            s.step_unchecked(s.cfl_limit())
+        ind = TroubledCellIndicator(seed=0)
+        ind.collect(s, 1e-4)
+        counts.append(ind.evaluate(0.0, holdout=0)["positives"])
+    assert counts[0] > 0 and counts[0] == counts[1], counts
