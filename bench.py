@@ -431,7 +431,8 @@ def main():
         timed3(max(a.warmup, 3))
         dist.barrier()
         tl = dist.reduce(timed3(a.steps), "max")
-        s3.step_unchecked(s3.cfl_limit())  # matches the profiled plain step
+        ph3 = (ctypes.c_double * 8)()
+        _native.check(L.qmhd_solver_profile_step(s3._h, ph3, 8))  # matches the profiled plain step
         fx, fy = learned_face_counts(s3)
         nfaces = (a.n + 1) * (a.n + 2 * ics.nghost(a.order))
         r_plain = s.state_component_to_host("rho")
@@ -439,6 +440,8 @@ def main():
         l1 = float(np.sum(np.abs(r_learn - r_plain)) / np.sum(np.abs(r_plain)))
         learned = {"value": zones * a.steps * WORLD / (tl * 1e-3), "unit": "zone-updates/s",
                    "ms_per_step": tl / a.steps, "speedup_vs_plain": t_ms / tl,
+                   "phase_ms_per_step": {k: round(v, 4) for k, v in zip(PHASES, list(ph3))},
+                   "phase_note": "control holds the indicator inference and the face lists",
                    "indicator": f"quasar_b200/data/indicator_mp{a.order}.npz",
                    "threshold": thr, "full_path_face_fraction": (fx + fy) / (2.0 * nfaces),
                    "rho_l1_vs_plain": l1, "steps_compared": max(a.warmup, 3) + a.steps + 1,

@@ -19,7 +19,8 @@ extern "C" {
 int qmhd_solver_time_auto_steps(qmhd_solver* solver, int steps, double* ms, int* done);
 
 /* One step with per-phase device times in ms (n >= QMHD_PROFILE_PHASES):
- * 0 control (step begin, dt), 1 reconstruction, 2 face flux, 3 cell EMF,
+ * 0 control (step begin, dt; with an indicator attached also its inference
+ * and the face lists), 1 reconstruction, 2 face flux, 3 cell EMF,
  * 4 corner EMF, 5 update, 6 ghost fill, 7 collocation + admissibility. */
 int qmhd_solver_profile_step(qmhd_solver* solver, double* ms_by_phase, int n);
 

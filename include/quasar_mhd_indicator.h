@@ -55,9 +55,15 @@ int qmhd_indicator_gradient(qmhd_indicator* ind, const float* features,
  * learned step's fast path reproduces the plain step within tol.  (The
  * early-accept test of numerics/mp_limiter.hpp:84-106 alone fails in nearly
  * every cell: near-constant fields fail it by sign noise while the limiter
- * moves them by rounding only.) */
+ * moves them by rounding only.)  A negative tol selects the literal label
+ * instead: 1 when the MP limiter fired (changed the unlimited value, the
+ * negation of the early accept of mp_limiter.hpp:84-106) on any
+ * characteristic field of such a face state. */
 int qmhd_indicator_collect(qmhd_indicator* ind, qmhd_solver* solver, float tol);
 long long qmhd_indicator_rows(const qmhd_indicator* ind);
+/* The collected labels (n = qmhd_indicator_rows bytes, collection order:
+ * per collected state its interior cells row by row). */
+int qmhd_indicator_labels(const qmhd_indicator* ind, unsigned char* labels, long long n);
 int qmhd_indicator_clear(qmhd_indicator* ind);
 
 /* Adam (beta 0.9 / 0.999) over random 128-row tiles, `tiles_per_step` tiles

@@ -32,6 +32,7 @@ BATCH_EXPORTS = ("qmhd_batch_create", "qmhd_batch_destroy", "qmhd_batch_size", "
 INDICATOR_EXPORTS = ("qmhd_indicator_create", "qmhd_indicator_destroy", "qmhd_indicator_get_params",
                      "qmhd_indicator_set_params", "qmhd_indicator_forward",
                      "qmhd_indicator_gradient", "qmhd_indicator_collect", "qmhd_indicator_rows",
+                     "qmhd_indicator_labels",
                      "qmhd_indicator_clear", "qmhd_indicator_train", "qmhd_indicator_evaluate",
                      "qmhd_indicator_threshold_for_recall", "qmhd_solver_set_indicator",
                      "qmhd_solver_learned_face_counts", "qmhd_batch_set_indicator")
@@ -117,6 +118,7 @@ def lib() -> ctypes.CDLL:
     L.qmhd_indicator_collect.argtypes = [vp, vp, ctypes.c_float]
     L.qmhd_indicator_rows.argtypes = [vp]
     L.qmhd_indicator_rows.restype = ctypes.c_longlong
+    L.qmhd_indicator_labels.argtypes = [vp, vp, ctypes.c_longlong]
     L.qmhd_indicator_clear.argtypes = [vp]
     L.qmhd_indicator_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                        ctypes.c_float, ctypes.c_int, ctypes.c_ulonglong, dp]

@@ -386,6 +386,14 @@ int qmhd_indicator_collect(qmhd_indicator* ind, qmhd_solver* solver, float tol) 
 
 long long qmhd_indicator_rows(const qmhd_indicator* ind) { return ind ? ind->impl.rows() : -1; }
 
+int qmhd_indicator_labels(const qmhd_indicator* ind, unsigned char* labels, long long n) {
+  return guarded([&] {
+    need(ind);
+    need(labels);
+    ind->impl.labels_to_host(labels, n);
+  });
+}
+
 int qmhd_indicator_clear(qmhd_indicator* ind) {
   return guarded([&] {
     need(ind);

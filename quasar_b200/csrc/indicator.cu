@@ -1011,9 +1011,12 @@ void Indicator::ensure_capacity(long long rows) {
 
 // Feature rows and limiter labels of every interior cell of a live state
 // (the solver's own reconstruction run once per direction with recording):
-// label 1 where a limited face state departs by more than `tol`.
+// label 1 where a limited face state departs by more than `tol`, or, for a
+// negative tol, where the limiter fired on any characteristic field.
 void Indicator::collect(const StageArgs& a, cudaStream_t solver_stream, float tol) {
-  if (!(tol >= 0.0f)) throw std::invalid_argument("indicator: label tolerance must be >= 0");
+  if (tol != tol) throw std::invalid_argument("indicator: label tolerance is NaN");
+  const int literal = tol < 0.0f ? 1 : 0;
+  if (literal) tol = 0.0f;
   if (a.order != 5 && a.order != 7)
     throw std::invalid_argument("indicator: training data needs an mp5 or mp7 solver");
   const Grid& g = a.g;
@@ -1031,8 +1034,8 @@ void Indicator::collect(const StageArgs& a, cudaStream_t solver_stream, float to
   ick(cudaStreamWaitEvent(stream_, ev, 0), "event wait");
   cudaEventDestroy(ev);
   ick(cudaMemsetAsync(label_, 0, sizeof(int) * size_t(g.size()), stream_), "labels");
-  launch_reconstruct_label(a, 0, label_, stream_);
-  launch_reconstruct_label(a, 1, label_, stream_);
+  launch_reconstruct_label(a, 0, label_, literal, stream_);
+  launch_reconstruct_label(a, 1, label_, literal, stream_);
   unsigned char* bad = nullptr;
   ick(cudaMalloc(&bad, size_t(n)), "bad rows");
   launch_cell_features(g, a.u, a.gamma, xs_ + size_t(rows_) * kFeatPad, bad, stream_);
@@ -1041,6 +1044,15 @@ void Indicator::collect(const StageArgs& a, cudaStream_t solver_stream, float to
   ick(cudaStreamSynchronize(stream_), "collect");
   cudaFree(bad);
   rows_ += n;
+}
+
+void Indicator::labels_to_host(unsigned char* out, long long n) const {
+  if (n != rows_)
+    throw std::invalid_argument("indicator: labels buffer holds " + std::to_string(n) +
+                                " rows, " + std::to_string(rows_) + " collected");
+  if (n == 0) return;
+  ick(cudaMemcpyAsync(out, ys_, size_t(n), cudaMemcpyDeviceToHost, stream_), "labels to host");
+  ick(cudaStreamSynchronize(stream_), "labels to host");
 }
 
 double Indicator::train(int epochs, int tiles_per_step, float lr, float pos_weight, int holdout,

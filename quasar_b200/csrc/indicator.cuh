@@ -108,6 +108,8 @@ class Indicator {
   // from solver states (MhdSolver2D::live_args).
   void collect(const StageArgs& live, cudaStream_t solver_stream, float tol);
   long long rows() const { return rows_; }
+  // Copy the collected labels (one byte per row, collection order) to host.
+  void labels_to_host(unsigned char* out, long long n) const;
   void clear_rows() { rows_ = 0; }
   // Adam over random 128-row tiles of the training rows; one tile in
   // `holdout` (chosen by a hash of its index) is held out (0 = none).

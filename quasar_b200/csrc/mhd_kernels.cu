@@ -533,7 +533,7 @@ constexpr size_t kReconSmem = 98 * kReconThreads * sizeof(double);
 
 template <int DIR, int H>
 __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, double gamma, St& ul,
-                             St& ur) {
+                             St& ur, bool* fired_l = nullptr, bool* fired_r = nullptr) {
   constexpr int S = 2 * H + 2, W = 2 * H + 1;
   const St cl = load_cell(u, k0 - step), cr = load_cell(u, k0);
   St ref;
@@ -635,9 +635,11 @@ __device__ void mp_pair_loop(const StateP& u, long long k0, long long step, doub
 #pragma unroll
     for (int s = 0; s < W; ++s) win[s] = ch[s];
     const double wl = mp_recon<W>(win, f);
+    if (fired_l && f) *fired_l = true;
 #pragma unroll
     for (int s = 0; s < W; ++s) win[s] = ch[W - s];
     const double wr = mp_recon<W>(win, f);
+    if (fired_r && f) *fired_r = true;
     double Rc[7];
     if (usable) {
 #pragma unroll
@@ -1093,7 +1095,9 @@ struct FaceList {
 // 2: the unlimited component-wise path; a face whose unlimited states are
 // not admissible is appended to `defer` for the characteristic pass that
 // follows (the plain step's path for it, fallbacks included) unless it is
-// listed already.  Orders 1 and 2 ignore MODE.
+// listed already; 3: the characteristic path, recording per cell whether the
+// MP limiter fired on any characteristic field of a state whose stencil is
+// centred on it (label[cell] = 1).  Orders 1 and 2 ignore MODE.
 template <int DIR, int ORDER, int MODE>
 __device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const IfaceP& out,
                                            double gamma, int i, int j, int* label,
@@ -1116,7 +1120,14 @@ __device__ __forceinline__ void recon_face(const Grid& g, const StateP& u, const
         return;
       }
     } else {
-      mp_pair_loop<DIR, H>(u, k0, step, gamma, ul, ur);
+      bool fl = false, fr = false;
+      mp_pair_loop<DIR, H>(u, k0, step, gamma, ul, ur, &fl, &fr);
+      if (MODE == 3) {
+        // the literal label: the MP limiter fired on some characteristic
+        // field of the state whose stencil is centred on the cell
+        if (fl) atomicMax(label + (k0 - step), 1);
+        if (fr) atomicMax(label + k0, 1);
+      }
       if (MODE == 1) {
         St ll, lr;
         mp_pair_lin<DIR, H>(u, k0, step, ll, lr);
@@ -1193,12 +1204,17 @@ __global__ void __launch_bounds__(128, 4) k_reconstruct(Grid g, StateP u, IfaceP
   b_reconstruct<DIR, ORDER>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y);
 }
 
-// Limiter labels of the cells (training data of the indicator).
+// Limiter labels of the cells (training data of the indicator): the
+// departure of the limited states (literal = 0) or whether the limiter fired
+// (literal = 1).
 template <int DIR, int ORDER>
 __global__ void __launch_bounds__(128) k_reconstruct_label(Grid g, StateP u, IfaceP out,
                                                            double gamma, const Ctl* ctl,
-                                                           int* label) {
-  b_reconstruct<DIR, ORDER, 1>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y, label);
+                                                           int* label, int literal) {
+  if (literal)
+    b_reconstruct<DIR, ORDER, 3>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y, label);
+  else
+    b_reconstruct<DIR, ORDER, 1>(g, u, out, gamma, ctl, blockIdx.x, blockIdx.y, label);
 }
 
 // Learned mode, pass 1: every face by the unlimited component-wise path
@@ -2740,14 +2756,15 @@ dim3 recon_grid(const Grid& g) {
 }
 }  // namespace
 
-void launch_reconstruct_label(const StageArgs& a, int dir, int* label, cudaStream_t s) {
+void launch_reconstruct_label(const StageArgs& a, int dir, int* label, int literal,
+                              cudaStream_t s) {
   const dim3 block(kBX, 4);
   const IfaceP out = dir == 0 ? a.ix : a.iy;
 #define QB_LBL(D, O)                                                                          \
   if (dir == D && a.order == O) {                                                            \
     ensure_smem((const void*)k_reconstruct_label<D, O>, kReconSmem);                          \
     return (void)k_reconstruct_label<D, O><<<recon_grid<D, O>(a.g), block, kReconSmem, s>>>( \
-        a.g, a.u, out, a.gamma, a.ctl, label);                                                \
+        a.g, a.u, out, a.gamma, a.ctl, label, literal);                                       \
   }
   QB_LBL(0, 5) QB_LBL(1, 5) QB_LBL(0, 7) QB_LBL(1, 7)
 #undef QB_LBL

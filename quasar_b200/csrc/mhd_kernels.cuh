@@ -277,7 +277,8 @@ void launch_batch_ctl(const BatchRec* r, int n, int what, double t, double t_end
 // face state of a stencil centred on the cell, limited in characteristic
 // fields, departs from the unlimited component-wise state, relative to the
 // state's scale.  The array must start at zero.
-void launch_reconstruct_label(const StageArgs& a, int dir, int* label, cudaStream_t s);
+void launch_reconstruct_label(const StageArgs& a, int dir, int* label, int literal,
+                              cudaStream_t s);
 // Unlimited component-wise reconstruction of every face, then the full
 // characteristic path for the listed faces (count on the device).  Faces
 // whose unlimited states are not admissible are appended to the list (flag:

@@ -217,6 +217,7 @@ void MhdSolver2D::front_impl(int order, int dt_mode, int anchor_mode) {
                         ind_status_, stream_),
        "indicator launch");
     launch_face_lists(g_, flags_, flists_, flists_ + g_.size(), fcounts_, stream_);
+    mark(0);
   }
   reconstruct_stage(a, order);
   mark(1);

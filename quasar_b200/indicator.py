@@ -58,11 +58,19 @@ class TroubledCellIndicator:
     def collect(self, solver, tol: float = 1e-6) -> None:
         """Append the solver's live state: features, and labels 1 where a
         limited face state departs from the unlimited component-wise one by
-        more than `tol` of the state's scale."""
+        more than `tol` of the state's scale (a negative tol: where the MP
+        limiter fired on any characteristic field, the literal label)."""
         _native.check(_native.lib().qmhd_indicator_collect(self._h, solver._h, ctypes.c_float(tol)))
 
     def rows(self) -> int:
         return int(_native.lib().qmhd_indicator_rows(self._h))
+
+    def labels(self) -> np.ndarray:
+        """The collected labels, one per row in collection order (per state
+        its interior cells row by row)."""
+        out = np.empty(self.rows(), dtype=np.uint8)
+        _native.check(_native.lib().qmhd_indicator_labels(self._h, out.ctypes.data, out.size))
+        return out
 
     def clear(self) -> None:
         _native.check(_native.lib().qmhd_indicator_clear(self._h))

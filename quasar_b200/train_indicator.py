@@ -143,6 +143,100 @@ def inference_report(n=2048, order=5, t_develop=0.3, steps=100, snapshots=2, pat
             "div_b_rel_plain": plain.divergence_b_relative()}
 
 
+def _heuristic_scores(solver, n, order, gamma):
+    """Per interior cell (row by row): the largest relative density or
+    pressure jump over its 5 x 5 stencil, max |q / q_centre - 1| for
+    q = rho, p -- the cheap shock detector a troubled-cell indicator must beat."""
+    from numpy.lib.stride_tricks import sliding_window_view
+    ng = ics.nghost(order)
+    shape = (n + 2 * ng, n + 2 * ng)
+    st = {c: solver.state_component_to_host(c).reshape(shape) for c in ics.COMPONENTS}
+    rho = st["rho"]
+    bx = 0.5 * (st["bx_face"] + np.roll(st["bx_face"], -1, axis=1))
+    by = 0.5 * (st["by_face"] + np.roll(st["by_face"], -1, axis=0))
+    kin = 0.5 * (st["mx"] ** 2 + st["my"] ** 2 + st["mz"] ** 2) / rho
+    p = (gamma - 1.0) * (st["energy"] - kin - 0.5 * (bx * bx + by * by + st["bz_cell"] ** 2))
+    sl = slice(ng - 2, ng + n + 2)
+    score = np.zeros((n, n))
+    for q in (rho[sl, sl], p[sl, sl]):
+        win = sliding_window_view(q, (5, 5))          # (n, n, 5, 5)
+        c = q[2:-2, 2:-2][:, :, None, None]
+        score = np.maximum(score, np.abs(win / c - 1.0).max(axis=(2, 3)))
+    return score.reshape(-1)
+
+
+def _flagged_at_recall(scores, labels, recall):
+    """Fraction of cells flagged by the lowest threshold on `scores` (higher
+    = more troubled) that still flags `recall` of the positive labels."""
+    pos = np.sort(scores[labels == 1])
+    if pos.size == 0:
+        return 0.0, np.inf
+    thr = pos[int(np.floor((1.0 - recall) * pos.size))]
+    return float(np.mean(scores >= thr)), float(thr)
+
+
+def gain_report(n=512, order=5, t_develop=0.3, steps=60, recall=0.95, path=None):
+    """What the trained indicator gains on a developed flow (Orszag-Tang n^2,
+    plain step to t_develop): the fraction of cells each scorer must flag to
+    catch `recall` of the plain limiter's activations on that state -- the
+    shipped network, the same network untrained (its initial weights), and
+    the density/pressure jump heuristic -- with the density L1 gap of the
+    learned step at the shipped network's threshold after `steps` steps, and
+    the recall of the shipped flags against the literal label (the limiter
+    fired on any characteristic field) beside the training label."""
+    ind, thr_shipped = load(path, order)
+    z = np.load(path or default_path(order))
+    tol = float(json.loads(str(z["meta"])).get("tol", 1e-4))
+    gamma = 5.0 / 3.0
+    solvers = []
+    for _ in range(2):
+        s = _solver(n, order, 0)
+        for name, arr in zip(ics.COMPONENTS, ics.orszag_tang(n, order=order)):
+            s.seed_state(name, arr)
+        t, taken = s.advance_auto(0.0, t_develop, 10 ** 7)
+        solvers.append(s)
+    plain, learned = solvers
+    out = {"workload": f"Orszag-Tang {n}^2 MP{order}, periodic, developed to t={t:.4f} "
+                       f"({taken} plain steps)", "recall": recall, "label_tol": tol}
+    trained = TroubledCellIndicator(seed=0)
+    trained.set_params(ind.params())
+    untrained = TroubledCellIndicator(seed=0)
+    for name, net in (("trained", trained), ("untrained", untrained)):
+        net.collect(plain, tol)
+        thr = net.threshold_for_recall(recall, holdout=0)
+        ev = net.evaluate(thr, holdout=0)
+        out[name] = {"flagged": ev["flagged"], "recall": ev["recall"], "threshold": thr}
+    labels = trained.labels()
+    out["positives"] = int(labels.sum())
+    out["cells"] = int(labels.size)
+    flagged, thr = _flagged_at_recall(_heuristic_scores(plain, n, order, gamma), labels, recall)
+    out["heuristic"] = {"flagged": flagged, "threshold": thr,
+                        "score": "max over the 5x5 stencil of |rho/rho_c - 1| and |p/p_c - 1|"}
+    # the shipped threshold on this state, against both labels
+    out["shipped_threshold"] = thr_shipped
+    out["shipped_recall_training_label"] = trained.evaluate(thr_shipped, holdout=0)["recall"]
+    literal = TroubledCellIndicator(seed=0)
+    literal.set_params(ind.params())
+    literal.collect(plain, -1.0)
+    lev = literal.evaluate(thr_shipped, holdout=0)
+    out["literal_label"] = {"positive_fraction": lev["positives"] / max(lev["total"], 1),
+                            "shipped_recall": lev["recall"], "flagged": lev["flagged"]}
+    # the learned step at the shipped threshold against the plain step
+    ind.attach(learned, thr_shipped)
+    for _ in range(steps):
+        dt = plain.cfl_limit()
+        plain.step_unchecked(dt)
+        learned.step_unchecked(dt)
+    ng = ics.nghost(order)
+    sl = (slice(ng, ng + n), slice(ng, ng + n))
+    shape = (n + 2 * ng, n + 2 * ng)
+    rp = plain.state_component_to_host("rho").reshape(shape)[sl]
+    rl = learned.state_component_to_host("rho").reshape(shape)[sl]
+    out["rho_l1_vs_plain"] = float(np.sum(np.abs(rl - rp)) / np.sum(np.abs(rp)))
+    out["steps"] = steps
+    return out
+
+
 def default_path(order):
     return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", f"indicator_mp{order}.npz")
 
