@@ -9,9 +9,11 @@ auto-dt SSP-RK3 step (cfl_limit + step), dt kept on the device.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--case rotor|blast]
                     [--n 4096] [--impl b200|reference]
 
-N > 1 (torchrun, one process per GPU) runs N independent replicas (the
-single-instance step is not domain-decomposed here); the value is the sum over
-ranks with the time taken as the max over ranks.
+N > 1 (torchrun, one process per GPU): the headline single-instance step
+runs as N independent replicas (it is not domain-decomposed here); the batched
+lines split their independent instances over the ranks, zones balanced
+(quasar_b200/shard.py), with no data-path exchange.  Either way the value is
+the zone-updates summed over ranks over the time taken as the max over ranks.
 
 Printed JSON line: value = device-timed zone-updates/s with the state resident
 in HBM; e2e = the same metric through the public C ABI with host buffers
@@ -457,22 +459,27 @@ def main():
     batched = combined = None
     if not a.no_batch:
         kb = max(10, a.steps // 10)
-        insts = ics.batch_instances(count=256, seed=0, order=5)
+        from quasar_b200 import shard
+        every = ics.batch_instances(count=256, seed=0, order=5)
+        # instance-parallel over the ranks: each steps its share, no exchange
+        insts = shard.rank_share(every, [x["nx"] * x["ny"] for x in every], RANK, WORLD)
         b = make_batch(insts, 5)
         ctas, trials = b.autotune()
         b.time_steps(3)
         bms, bzu = b.time_steps(kb)
-        bms = dist.reduce(bms, "max")
+        bms, bzu = dist.reduce(bms, "max"), dist.reduce(bzu, "sum")
         del b
         seq_ms, seq_zu = sequential_instances(insts, kb)
-        seq_ms = dist.reduce(seq_ms, "max")
+        seq_ms, seq_zu = dist.reduce(seq_ms, "max"), dist.reduce(seq_zu, "sum")
         batched = {"workload": "256 seeded MP5 instances, sides log-uniform in [64, 512], "
                                "Orszag-Tang / oblique Brio-Wu / linear fast or Alfven waves",
-                   "zones": sum(x["nx"] * x["ny"] for x in insts),
-                   "value": bzu * WORLD / (bms * 1e-3), "unit": "zone-updates/s",
+                   "zones": sum(x["nx"] * x["ny"] for x in every),
+                   "value": bzu / (bms * 1e-3), "unit": "zone-updates/s",
+                   "parallelism": f"instance-parallel over {WORLD} rank(s), zones balanced "
+                                  "(quasar_b200/shard.py); zone-updates summed, time max",
                    "ms_per_step": bms / kb, "autotuned_ctas_per_sm": ctas,
                    "autotune_steps": trials,
-                   "sequential": {"value": seq_zu * WORLD / (seq_ms * 1e-3),
+                   "sequential": {"value": seq_zu / (seq_ms * 1e-3),
                                   "ms_per_step": seq_ms / kb,
                                   "how": "the same instances stepped one after another, each "
                                          "its own solver's device-resident graph loop of the "
@@ -481,7 +488,9 @@ def main():
         if not a.no_learned:
             from quasar_b200 import train_indicator
             from quasar_b200.indicator import attach_batch
-            b = make_batch(ics.combined_instances(seed=2, order=7), 7)
+            every = ics.combined_instances(seed=2, order=7)
+            mine = shard.rank_share(every, [x["nx"] * x["ny"] for x in every], RANK, WORLD)
+            b = make_batch(mine, 7)
             ctas, trials = b.autotune()
             b.time_steps(3)
             pms, pzu = b.time_steps(kb)
@@ -490,11 +499,12 @@ def main():
             b.time_steps(3)
             lms, lzu = b.time_steps(kb)
             pms, lms = dist.reduce(pms, "max"), dist.reduce(lms, "max")
+            pzu, lzu = dist.reduce(pzu, "sum"), dist.reduce(lzu, "sum")
             combined = {"workload": "one batch: Orszag-Tang 8192^2 MP7 + 64 seeded rotor/blast MP7 "
                                     "instances, sides log-uniform in [256, 1024]",
-                        "zones": b.zones(), "unit": "zone-updates/s",
-                        "plain_batched": pzu * WORLD / (pms * 1e-3),
-                        "learned_batched": lzu * WORLD / (lms * 1e-3),
+                        "zones": sum(x["nx"] * x["ny"] for x in every), "unit": "zone-updates/s",
+                        "plain_batched": pzu / (pms * 1e-3),
+                        "learned_batched": lzu / (lms * 1e-3),
                         "speedup": (lzu / lms) / (pzu / pms),
                         "ms_per_step_plain": pms / kb, "ms_per_step_learned": lms / kb,
                         "note": "plain steps first, then the learned steps continue the same "
