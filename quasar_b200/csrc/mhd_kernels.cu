@@ -19,6 +19,9 @@
 // (or many) runs without a host round trip and can be captured in a graph.
 #include "mhd_device.cuh"
 #include "mhd_kernels.cuh"
+#include "tc.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
@@ -1755,29 +1758,92 @@ __global__ void __launch_bounds__(128) k_cell_emf(Grid g, StateP u, double* cell
 // cell than 32x8 (22/16 against 14/8 at MP7).
 constexpr int kCellTX = 16, kCellTY = 16;
 
-template <int ORDER>
+// TMA staging of the tile: rows of kTmaBW doubles (192 bytes) starting one
+// cell left of the stencil's first column, so that the innermost coordinate
+// of every copy is even (16-byte aligned); planes of SY rows are multiples of
+// 128 bytes at both orders.
+constexpr int kTmaBW = 24;
+
+template <int ORDER, bool TMA = false>
 constexpr int cell_smem_doubles() {
-  return 8 * (kCellTY + 2 * (ORDER == 7 ? 3 : 2)) *
-         ((kCellTX + 2 * (ORDER == 7 ? 3 : 2)) + kCellTX);
+  constexpr int H = ORDER == 7 ? 3 : 2, SY = kCellTY + 2 * H;
+  // TMA: 16 more doubles so that the staged planes can start on 128 bytes
+  return 8 * SY * (TMA ? kTmaBW : kCellTX + 2 * H) + 8 * SY * kCellTX + (TMA ? 16 : 0);
 }
 
-template <int ORDER>
+// 3-D tiled TMA load of one box into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
+                                            int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(tc::smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(tc::smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// TMA: the eight state planes of the tile come in by one TMA copy each
+// (issued by one thread, completing on an mbarrier whose wait is bounded)
+// from `map`, the register's 3-D tensor map; out-of-range cells are filled
+// with zeros by the copy, as the plain staging does.
+template <int ORDER, bool TMA = false>
 __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, double* cell_ez,
                                              const double* xs, const double* ys, int cfl_reduce,
-                                             double gamma, Ctl* ctl, int bx, int by) {
+                                             double gamma, Ctl* ctl, int bx, int by,
+                                             const CUtensorMap* map = nullptr) {
   constexpr int H = ORDER == 7 ? 3 : 2, N = 2 * H + 1, Q = ORDER == 7 ? 4 : 3;
   constexpr int TX = kCellTX, TY = kCellTY, SX = TX + 2 * H, SY = TY + 2 * H;
-  extern __shared__ double sm[];
-  double* S = sm;                // [8][SY][SX] staged state
-  double* X = sm + 8 * SY * SX;  // [8][SY][TX] x-recovered rows of one x-node
+  // row stride and column offset of the staged tile: S[c][r][x] is the
+  // stencil cell (i0 - H + x, j0 - H + r) at S + (c * SY + r) * RS + XO + x
+  constexpr int RS = TMA ? kTmaBW : SX, XO = TMA ? 1 : 0;
+  static_assert(!TMA || (SX + XO <= kTmaBW && (SY * kTmaBW * 8) % 128 == 0), "TMA box");
+  extern __shared__ __align__(128) double sm[];
+  // TMA destinations start on 128 bytes
+  double* S = TMA ? reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(sm) + 127) &
+                                              ~uintptr_t(127))
+                  : sm;          // [8][SY][RS] staged state
+  double* X = S + 8 * SY * RS;  // [8][SY][TX] x-recovered rows of one x-node
   __shared__ int s_stop;
   __shared__ double s_max[8];
+  __shared__ uint64_t s_bar;
   const int tid = threadIdx.y * TX + threadIdx.x;
   if (tid == 0) s_stop = ctl->status;
   __syncthreads();
   if (s_stop) return;
   const int i0 = bx * TX, j0 = by * TY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  if constexpr (TMA) {
+    // padded coordinates: x0 = i0 - H + ng - XO is even because ng - H = 1
+    // at both orders and i0 is a multiple of 16
+    if (tid == 0) {
+      tc::mbar_init(&s_bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      mbar_expect_tx(&s_bar, uint32_t(8 * SY * kTmaBW * sizeof(double)));
+      const int x0 = i0 - H + g.ng - XO, y0 = j0 - H + g.ng;
+      constexpr int kZ[8] = {0, 1, 2, 3, 4, 8, 9, 7};  // rho..E, bxc, byc, bz
+#pragma unroll
+      for (int c = 0; c < 8; ++c) tma_load_3d(S + c * SY * kTmaBW, map, x0, y0, kZ[c], &s_bar);
+    }
+    __syncthreads();  // the barrier is initialised before anyone waits on it
+    // one warp polls the mbarrier; the others sleep in the block barrier,
+    // which also orders the landed tile before their reads
+    bool arrived = true;
+    if (tid < 32) arrived = tc::mbar_wait(&s_bar, 0);
+    if (!__syncthreads_and(arrived ? 1 : 0)) {
+      // the copies did not land in time: report it, give them a second
+      // bounded wait so that none is still writing when the block exits
+      if (tid == 0) {
+        atomicOr(&ctl->status, kStatusWaitExpired);
+        tc::mbar_wait(&s_bar, 0);
+      }
+      __syncthreads();
+      return;
+    }
+  } else {
   // staging: one index computation per staged cell, its 8 components
   // loaded with the same offset
   for (int r = threadIdx.y; r < SY; r += TY) {
@@ -1794,6 +1860,7 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
     }
   }
   __syncthreads();
+  }
   const bool phx = g.bc[1] != 0, phy = g.bc[3] != 0;
   const bool active =
       i <= g.nx && j <= g.ny && !((i == g.nx && !phx) || (j == g.ny && !phy));
@@ -1810,7 +1877,7 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
 #pragma unroll
     for (int m = 0; m < 8 * SY / TY; ++m) {
       const int t = threadIdx.y + m * TY;
-      const double* row = S + t * SX + threadIdx.x;
+      const double* row = S + t * RS + XO + threadIdx.x;
       double smp[N];
 #pragma unroll
       for (int q = 0; q < N; ++q) smp[q] = row[q];
@@ -1872,6 +1939,18 @@ __global__ void __launch_bounds__(256, 3) k_cell_emf_s(Grid g, StateP u, double*
                                                     const double* xs, const double* ys,
                                                     int cfl_reduce, double gamma, Ctl* ctl) {
   b_cell_emf_s<ORDER>(g, u, cell_ez, xs, ys, cfl_reduce, gamma, ctl, blockIdx.x, blockIdx.y);
+}
+
+// The same with the tile staged by TMA from the register's tensor map
+// (single-instance path; this GPU's own memory, no multicast).
+template <int ORDER>
+__global__ void __launch_bounds__(256, 3) k_cell_emf_tma(Grid g, StateP u,
+                                                      const __grid_constant__ CUtensorMap map,
+                                                      double* cell_ez, const double* xs,
+                                                      const double* ys, int cfl_reduce,
+                                                      double gamma, Ctl* ctl) {
+  b_cell_emf_s<ORDER, true>(g, u, cell_ez, xs, ys, cfl_reduce, gamma, ctl, blockIdx.x,
+                            blockIdx.y, &map);
 }
 
 // Face -> edge interpolation (mhd_ct.hip:50-97) with the constant shortcut.
@@ -2106,6 +2185,87 @@ __device__ __forceinline__ void b_update(const Grid& g, const StateP& un, const 
   if (i < g.nx) {
     const double d = __dadd_rn(div_by(ez[k + 1], g.dx, rdx), div_by(-ez[k], g.dx, rdx));
     out.c[6][k] = combine(un.c[6][k], b == 0.0 ? 0.0 : us.c[6][k], d);
+  }
+}
+
+// b_update two cells at a time, every load and store of the pair one
+// 16-byte double2 access (the pair's first padded column is even and the
+// pitch is even, so each pair is aligned); the per-cell arithmetic and the
+// cells written are b_update's.  Reads of the pair's partner beyond the
+// updated range stay inside the padded arrays (ng >= 3).
+__device__ __forceinline__ double2 ld2(const double* p) {
+  return __ldg(reinterpret_cast<const double2*>(p));
+}
+__device__ __forceinline__ void st_pair(double* p, bool a, bool b, double va, double vb) {
+  if (a && b) *reinterpret_cast<double2*>(p) = make_double2(va, vb);
+  else if (a) p[0] = va;
+  else if (b) p[1] = vb;
+}
+__global__ void __launch_bounds__(256) k_update2(Grid g, StateP un, StateP us, StateP out,
+                                                 FluxP fx, FluxP fy, const double* ez,
+                                                 const double* dt_dev, double dt_host, int stage,
+                                                 const Ctl* ctl) {
+  const int pr = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ia = 2 * pr - g.ng;  // the pair is cells ia, ia + 1 (padded columns 2 pr, 2 pr + 1)
+  if (ia > g.nx || j > g.ny) return;
+  if (ctl->status) return;
+  const double dt = dt_dev ? *dt_dev : dt_host;
+  double a, b, c;
+  if (stage == 0) {
+    a = 1.0; b = 0.0; c = dt;
+  } else if (stage == 1) {
+    a = 3.0 / 4.0; b = 1.0 / 4.0; c = (1.0 / 4.0) * dt;
+  } else {
+    a = 1.0 / 3.0; b = 2.0 / 3.0; c = (2.0 / 3.0) * dt;
+  }
+  auto combine = [&](double vn, double vs, double d) {
+    if (b == 0.0) return __dadd_rn(__dmul_rn(a, vn), __dmul_rn(c, d));
+    return crsum3(__dmul_rn(a, vn), __dmul_rn(b, vs), __dmul_rn(c, d));
+  };
+  const long long k = g.idx(ia, j), P = g.pitch;
+  const double rdx = pow2_recip(g.dx), rdy = pow2_recip(g.dy);
+  const int ib = ia + 1;
+  // cell-centred components: i < nx, j < ny
+  const bool ca = j < g.ny && ia >= 0 && ia < g.nx, cb = j < g.ny && ib >= 0 && ib < g.nx;
+  if (ca || cb) {
+    const int cc[6] = {0, 1, 2, 3, 4, 7};
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      const int q = cc[t];
+      const double2 x01 = ld2(fx.f[q] + k);
+      const double x2 = __ldg(fx.f[q] + k + 2);
+      const double2 y0 = ld2(fy.f[q] + k), y1 = ld2(fy.f[q] + k + P);
+      const double dxa = __dadd_rn(div_by(x01.y, g.dx, rdx), div_by(-x01.x, g.dx, rdx));
+      const double dxb = __dadd_rn(div_by(x2, g.dx, rdx), div_by(-x01.y, g.dx, rdx));
+      const double dya = __dadd_rn(div_by(y1.x, g.dy, rdy), div_by(-y0.x, g.dy, rdy));
+      const double dyb = __dadd_rn(div_by(y1.y, g.dy, rdy), div_by(-y0.y, g.dy, rdy));
+      const double2 vn = ld2(un.c[q] + k);
+      const double2 vs = b == 0.0 ? make_double2(0.0, 0.0) : ld2(us.c[q] + k);
+      st_pair(out.c[q] + k, ca, cb, combine(vn.x, vs.x, __dadd_rn(-dxa, -dya)),
+              combine(vn.y, vs.y, __dadd_rn(-dxb, -dyb)));
+    }
+  }
+  const double2 e0 = ld2(ez + k);
+  // x-face field: i <= nx, j < ny
+  const bool fa = j < g.ny && ia >= 0, fb = j < g.ny && ib >= 0 && ib <= g.nx;
+  if (fa || fb) {
+    const double2 e1 = ld2(ez + k + P);
+    const double2 vn = ld2(un.c[5] + k);
+    const double2 vs = b == 0.0 ? make_double2(0.0, 0.0) : ld2(us.c[5] + k);
+    const double da = __dadd_rn(div_by(-e1.x, g.dy, rdy), div_by(e0.x, g.dy, rdy));
+    const double db = __dadd_rn(div_by(-e1.y, g.dy, rdy), div_by(e0.y, g.dy, rdy));
+    st_pair(out.c[5] + k, fa, fb, combine(vn.x, vs.x, da), combine(vn.y, vs.y, db));
+  }
+  // y-face field: i < nx, j <= ny
+  const bool ha = ia >= 0 && ia < g.nx, hb = ib >= 0 && ib < g.nx;
+  if (ha || hb) {
+    const double e2 = __ldg(ez + k + 2);
+    const double2 vn = ld2(un.c[6] + k);
+    const double2 vs = b == 0.0 ? make_double2(0.0, 0.0) : ld2(us.c[6] + k);
+    const double da = __dadd_rn(div_by(e0.y, g.dx, rdx), div_by(-e0.x, g.dx, rdx));
+    const double db = __dadd_rn(div_by(e2, g.dx, rdx), div_by(-e0.y, g.dx, rdx));
+    st_pair(out.c[6] + k, ha, hb, combine(vn.x, vs.x, da), combine(vn.y, vs.y, db));
   }
 }
 
@@ -2505,6 +2665,14 @@ void launch_face_flux(const StageArgs& a, int dir, bool speeds, cudaStream_t s) 
 template <int ORDER>
 static void cell_tiled_launch(const StageArgs& a, bool cfl_reduce, cudaStream_t s) {
   const Grid& g = a.g;
+  const dim3 grid(cdiv(g.nx + 1, kCellTX), cdiv(g.ny + 1, kCellTY));
+  if (a.cell_map) {
+    constexpr size_t tbytes = sizeof(double) * cell_smem_doubles<ORDER, true>();
+    ensure_smem((const void*)k_cell_emf_tma<ORDER>, tbytes);
+    k_cell_emf_tma<ORDER><<<grid, dim3(kCellTX, kCellTY), tbytes, s>>>(
+        g, a.u, *a.cell_map, a.cell_ez, a.xspd, a.yspd, cfl_reduce ? 1 : 0, a.gamma, a.ctl);
+    return;
+  }
   constexpr size_t bytes = sizeof(double) * cell_smem_doubles<ORDER>();
   static bool configured = false;
   if (!configured) {
@@ -2512,7 +2680,6 @@ static void cell_tiled_launch(const StageArgs& a, bool cfl_reduce, cudaStream_t 
                          int(bytes));
     configured = true;
   }
-  const dim3 grid(cdiv(g.nx + 1, kCellTX), cdiv(g.ny + 1, kCellTY));
   k_cell_emf_s<ORDER><<<grid, dim3(kCellTX, kCellTY), bytes, s>>>(
       g, a.u, a.cell_ez, a.xspd, a.yspd, cfl_reduce ? 1 : 0, a.gamma, a.ctl);
 }
@@ -2532,6 +2699,36 @@ void launch_cell_emf(const StageArgs& a, bool cfl_reduce, cudaStream_t s) {
   }
 }
 
+bool make_state_tensor_map(const StateP& u, const Grid& g, int order, CUtensorMap* map) {
+  if (order != 5 && order != 7) return false;
+  const long long n = g.size();
+  if ((g.pitch & 1) || (n & 1)) return false;  // 16-byte strides
+  for (int c = 0; c < 8; ++c)
+    if (u.c[c] != u.c[0] + c * n) return false;
+  if (u.bxc != u.c[0] + 8 * n || u.byc != u.c[0] + 9 * n) return false;
+  if (reinterpret_cast<uintptr_t>(u.c[0]) & 15) return false;
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!encode) return false;
+  const int sy = kCellTY + 2 * (order == 7 ? 3 : 2);
+  cuuint64_t dims[3] = {cuuint64_t(g.pitch), cuuint64_t(g.ny + 2 * g.ng), 10};
+  cuuint64_t strides[2] = {cuuint64_t(g.pitch) * sizeof(double), cuuint64_t(n) * sizeof(double)};
+  cuuint32_t box[3] = {cuuint32_t(kTmaBW), cuuint32_t(sy), 1};
+  cuuint32_t elem[3] = {1, 1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, u.c[0], dims, strides, box, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 void launch_corner_emf(const StageArgs& a, cudaStream_t s) {
   const Grid& g = a.g;
   const dim3 block(kBX, 4);
@@ -2548,6 +2745,19 @@ void launch_update(const StageArgs& a, const StateP& un, const StateP& us, const
                    int stage, const double* dt_dev, double dt_host, cudaStream_t s) {
   const Grid& g = a.g;
   const dim3 block(kBX, 8);
+  // the paired form needs an even pitch, at least three ghost layers and
+  // 16-byte aligned arrays
+  bool pairs = (g.pitch % 2) == 0 && g.ng >= 3;
+  auto al = [](const double* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  for (int q = 0; q < 8 && pairs; ++q)
+    pairs = al(un.c[q]) && al(us.c[q]) && al(out.c[q]) && al(a.fx.f[q]) && al(a.fy.f[q]);
+  pairs = pairs && al(a.ez);
+  if (pairs) {
+    const dim3 grid(cdiv((g.nx + g.ng + 2) / 2, kBX), cdiv(g.ny + 1, 8));
+    k_update2<<<grid, block, 0, s>>>(g, un, us, out, a.fx, a.fy, a.ez, dt_dev, dt_host, stage,
+                                     a.ctl);
+    return;
+  }
   const dim3 grid(cdiv(g.nx + 1, kBX), cdiv(g.ny + 1, 8));
   k_update<<<grid, block, 0, s>>>(g, un, us, out, a.fx, a.fy, a.ez, dt_dev, dt_host, stage, a.ctl);
 }

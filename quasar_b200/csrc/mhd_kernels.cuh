@@ -2,6 +2,7 @@
 // Included by the kernels (.cu) and by the host solver.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -65,6 +66,7 @@ enum : int {
   kStatusNotSolenoidal = 4,  // live field fails the discrete div B preflight
   kStatusNotAdmissible = 8,  // live state inadmissible before a step
   kStatusDone = 16,          // device-resident loop reached t_end
+  kStatusWaitExpired = 32,   // a bounded device wait (TMA tile) ran out
 };
 
 struct StageArgs {
@@ -83,7 +85,17 @@ struct StageArgs {
   double* cell_ez;
   double* ez;      // corner EMF
   Ctl* ctl;
+  // TMA descriptor of the stage input's register (its ten arrays c[0..7],
+  // bxc, byc as one 3-D tensor), or null: the cell-EMF tile is then staged
+  // by plain loads
+  const CUtensorMap* cell_map = nullptr;
 };
+
+// The 3-D tensor map (x, y, array) of a state register whose ten arrays are
+// consecutive in memory, with the box the cell-EMF tile stages; false where
+// the layout or the TMA alignment rules do not allow one (odd pitch, orders
+// other than 5 and 7, or no driver entry point).
+bool make_state_tensor_map(const StateP& u, const Grid& g, int order, CUtensorMap* map);
 
 // Launch wrappers (mhd_kernels.cu).  All take a stream and never allocate.
 void launch_fill_ghosts(const Grid& g, const StateP& u, cudaStream_t s);

@@ -97,6 +97,7 @@ MhdSolver2D::MhdSolver2D(const Config& c) : cfg_(c) {
   ez_ = take();
   xnj_ = iarena_;
   ynj_ = iarena_ + n;
+  for (int k = 0; k < 5; ++k) tmap_ok_[k] = make_state_tensor_map(st_[k], g_, cfg_.order, &tmaps_[k]);
   Ctl init{};
   *ctl_host_ = init;
   ck(cudaMemcpyAsync(ctl_, ctl_host_, sizeof(Ctl), cudaMemcpyHostToDevice, stream_), "ctl init");
@@ -147,6 +148,8 @@ StageArgs MhdSolver2D::stage_args(const StateP& u, int order) const {
   a.cell_ez = cell_ez_;
   a.ez = ez_;
   a.ctl = ctl_;
+  for (int k = 0; k < 5; ++k)
+    if (u.c[0] == st_[k].c[0] && tmap_ok_[k]) a.cell_map = &tmaps_[k];
   return a;
 }
 

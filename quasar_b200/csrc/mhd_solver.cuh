@@ -118,6 +118,10 @@ class MhdSolver2D {
   unsigned long long* scalar_ = nullptr;
   int sum_blocks_ = 0;
   StateP st_[5];  // 0..3 rotating registers, 4 = request backup
+  // TMA descriptors of the registers (each register's ten arrays as one 3-D
+  // tensor) for the cell-EMF tile; tmap_ok_ false where none could be made
+  alignas(64) CUtensorMap tmaps_[5];
+  bool tmap_ok_[5] = {};
   int live_ = 0, s1_ = 1, s2_ = 2, next_ = 3;
   IfaceP ix_, iy_;
   FluxP fx_, fy_;
