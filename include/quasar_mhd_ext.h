@@ -27,6 +27,27 @@ int qmhd_solver_profile_step(qmhd_solver* solver, double* ms_by_phase, int n);
 /* Measured FP64 FMA throughput of the current device in TFLOP/s. */
 int qmhd_fp64_fma_peak(double* tflops);
 
+/* Tile hooks of a decomposed domain (quasar_b200/tiles.py), the pieces the
+ * reference's distributed runtime keeps inside its solver
+ * (src/distributed/mhd_runtime.cpp: dt and admissibility reduced over the
+ * owned cells, halos refreshed from the neighbours).
+ *
+ * qmhd_solver_set_owned_window: only interior cells [x0, x1) x [y0, y1)
+ * (0 <= x0 < x1 <= nx, 0 <= y0 < y1 <= ny) enter the reductions that decide
+ * dt (cfl_limit), positivity retries, the live-state preflights,
+ * divergence_b_max and conserved_cell_totals; the other cells are halo.
+ * The default window is every interior cell.
+ *
+ * qmhd_solver_write_halo: write a whole component (storage size, like
+ * qmhd_solver_seed_state) whose interior values are finite and come from
+ * the solver's own steps, e.g. the owned cells of neighbouring tiles: the
+ * state stays solver-owned, so its solenoidality preflight stays the one of
+ * a stepped state (a seeded state gets the stricter seeded-state test).
+ * Ghost layers need not be finite; they are closed again before use. */
+int qmhd_solver_set_owned_window(qmhd_solver* solver, int x0, int x1, int y0, int y1);
+int qmhd_solver_write_halo(qmhd_solver* solver, const char* component, const double* values,
+                           size_t n);
+
 /* Largest nx*ny accepted by qmhd_conserved_cell_totals_device. */
 #define QMHD_TOTALS_DEVICE_MAX_CELLS 67108864LL
 

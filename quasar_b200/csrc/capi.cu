@@ -151,6 +151,22 @@ int qmhd_solver_seed_state(qmhd_solver* s, const char* component, const double* 
   });
 }
 
+int qmhd_solver_set_owned_window(qmhd_solver* s, int x0, int x1, int y0, int y1) {
+  return guarded([&] {
+    need(s);
+    s->impl->set_owned_window(x0, x1, y0, y1);
+  });
+}
+
+int qmhd_solver_write_halo(qmhd_solver* s, const char* component, const double* values,
+                           size_t n) {
+  return guarded([&] {
+    need(s);
+    need(values);
+    s->impl->write_halo(component_index(component, false), values, (long long)n);
+  });
+}
+
 int qmhd_solver_state_component_to_host(qmhd_solver* s, const char* component, double* out,
                                         size_t n) {
   return guarded([&] {

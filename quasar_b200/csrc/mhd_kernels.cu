@@ -326,7 +326,7 @@ __device__ __forceinline__ void b_colloc_check(const Grid& g, const StateP& cand
                                      g.ny + g.ng - 1);
   cand.bxc[k] = bxc;
   cand.byc[k] = byc;
-  if (i < 0 || j < 0 || i >= g.nx || j >= g.ny) return;
+  if (i < 0 || j < 0 || i >= g.nx || j >= g.ny || !g.in_window(i, j)) return;
   const St b{cand.c[0][k], cand.c[1][k], cand.c[2][k], cand.c[3][k], cand.c[4][k], bxc, byc,
              cand.c[7][k]};
   if (has_base) {
@@ -1735,7 +1735,7 @@ __global__ void __launch_bounds__(128) k_cell_emf(Grid g, StateP u, double* cell
   }
   if (!cfl_reduce) return;
   double local = 0.0;
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.ny && g.in_window(i, j)) {
     const long long k = g.idx(i, j);
     const double r = (xs[k] + xs[k + 1]) + (ys[k] + ys[k + g.pitch]);
     local = isfinite(r) ? fmax(0.0, r) : kInf;
@@ -1919,7 +1919,7 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
   }
   if (!cfl_reduce) return;
   double local = 0.0;
-  if (i < g.nx && j < g.ny) {
+  if (i < g.nx && j < g.ny && g.in_window(i, j)) {
     const long long k = g.idx(i, j);
     const double r = (xs[k] + xs[k + 1]) + (ys[k] + ys[k + g.pitch]);
     local = isfinite(r) ? fmax(0.0, r) : kInf;
@@ -2351,7 +2351,7 @@ __global__ void k_step_end(Ctl* ctl) { k_step_end_body(ctl); }
 __global__ void k_divb_linf(Grid g, StateP u, unsigned long long* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= g.nx || j >= g.ny) return;
+  if (i >= g.nx || j >= g.ny || !g.in_window(i, j)) return;
   const long long k = g.idx(i, j);
   // ct_divb_linf_kernel (mhd_reduce.hip:505-553)
   const double rdx = pow2_recip(g.dx), rdy = pow2_recip(g.dy);
@@ -2371,6 +2371,7 @@ __global__ void k_cell_sums(Grid g, StateP u, double* partial) {
   for (long long t = blockIdx.x * (long long)blockDim.x + tid; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = int(t % g.nx), j = int(t / g.nx);
+    if (!g.in_window(i, j)) continue;
     const long long k = g.idx(i, j);
     double e;
     two_sum(s0, u.c[0][k], s0, e);

@@ -17,6 +17,14 @@ struct Grid {
   int nx, ny, ng, pitch;
   double dx, dy;
   int bc[4];
+  // Owned window [wx0, wx1) x [wy0, wy1) of interior cells: the reductions
+  // that decide dt, admissibility retries and the live-state preflights
+  // consider these cells only (a tile of a decomposed domain owns part of
+  // its interior; the rest is halo kept for the stencils).  Default: all.
+  int wx0 = 0, wx1 = 1 << 30, wy0 = 0, wy1 = 1 << 30;
+  __host__ __device__ bool in_window(int i, int j) const {
+    return i >= wx0 && i < wx1 && j >= wy0 && j < wy1;
+  }
   __host__ __device__ long long idx(int i, int j) const {
     return (long long)(i + ng) + (long long)pitch * (long long)(j + ng);
   }

@@ -173,6 +173,39 @@ void MhdSolver2D::seed_state(int comp, const double* host, long long n) {
   ck(cudaStreamSynchronize(stream_), "seed");
   seeded_dirty_ = true;
   solver_owned_ = false;
+  halo_write_ = false;
+  front_order_ = 0;
+}
+
+void MhdSolver2D::set_owned_window(int x0, int x1, int y0, int y1) {
+  if (!(0 <= x0 && x0 < x1 && x1 <= g_.nx && 0 <= y0 && y0 < y1 && y1 <= g_.ny))
+    throw std::invalid_argument("MhdSolver2D::set_owned_window: need 0 <= x0 < x1 <= nx and "
+                                "0 <= y0 < y1 <= ny");
+  g_.wx0 = x0;
+  g_.wx1 = x1;
+  g_.wy0 = y0;
+  g_.wy1 = y1;
+  release_graphs();  // the captured launches hold the grid by value
+  seeded_dirty_ = true;  // recompute the live preflights over the window
+  halo_write_ = solver_owned_;
+  front_order_ = 0;
+}
+
+void MhdSolver2D::write_halo(int comp, const double* host, long long n) {
+  if (comp < 0 || comp > 7) throw std::invalid_argument("MhdSolver2D: unknown state component");
+  if (n != g_.size())
+    throw std::invalid_argument("MhdSolver2D::write_halo: host buffer size mismatch");
+  // the interior must be finite; ghost layers are closed again before use
+  for (int j = 0; j < g_.ny; ++j)
+    for (int i = 0; i < g_.nx; ++i)
+      if (!std::isfinite(host[g_.idx(i, j)]))
+        throw std::invalid_argument("MhdSolver2D::write_halo: non-finite interior value");
+  ck(cudaMemcpyAsync(st_[live_].c[comp], host, sizeof(double) * n, cudaMemcpyHostToDevice,
+                     stream_),
+     "halo copy");
+  ck(cudaStreamSynchronize(stream_), "halo");
+  if (!seeded_dirty_) halo_write_ = solver_owned_;
+  seeded_dirty_ = true;
   front_order_ = 0;
 }
 
@@ -191,12 +224,17 @@ void MhdSolver2D::state_component_to_host(int comp, double* host, long long n) {
 // collocations, discrete div B).
 void MhdSolver2D::ensure_live_ready() {
   if (!seeded_dirty_) return;
+  // a state the solver stepped (here or on another tile, written back by
+  // write_halo) keeps the preflight of a stepped state; a seeded one gets
+  // the seeded-state test
+  const bool owned = halo_write_;
   launch_fill_ghosts(g_, st_[live_], stream_);
   launch_reset_stats(ctl_, stream_);
-  launch_colloc_check(g_, st_[live_], nullptr, 0, false, true, false, cfg_.gamma, ctl_, stream_);
+  launch_colloc_check(g_, st_[live_], nullptr, 0, false, true, owned, cfg_.gamma, ctl_, stream_);
   check_cuda("preflight launch");
   seeded_dirty_ = false;
-  solver_owned_ = false;
+  solver_owned_ = owned;
+  halo_write_ = false;
   front_order_ = 0;
 }
 

@@ -86,6 +86,15 @@ class MhdSolver2D {
   void learned_face_counts(long long* nx_faces, long long* ny_faces);
   cudaStream_t stream() const { return stream_; }
 
+  // Tile of a decomposed domain (quasar_b200/tiles.py).  The owned window
+  // [x0, x1) x [y0, y1) of interior cells restricts the reductions that
+  // decide dt, retries and the live-state preflights to the cells this tile
+  // owns.  write_halo writes a whole component like seed_state, but the
+  // values are the solver's own (stepped on another tile), so the state
+  // stays solver-owned and its preflight stays the one of a stepped state.
+  void set_owned_window(int x0, int x1, int y0, int y1);
+  void write_halo(int comp, const double* host, long long n);
+
  private:
   friend class MhdBatch2D;  // batched stage launches over the same registers
   struct Attempt {
@@ -122,6 +131,7 @@ class MhdSolver2D {
   // tensor) for the cell-EMF tile; tmap_ok_ false where none could be made
   alignas(64) CUtensorMap tmaps_[5];
   bool tmap_ok_[5] = {};
+  bool halo_write_ = false;  // the live state was last written by write_halo
   int live_ = 0, s1_ = 1, s2_ = 2, next_ = 3;
   IfaceP ix_, iy_;
   FluxP fx_, fy_;

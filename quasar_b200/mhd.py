@@ -219,6 +219,20 @@ class MhdSolver2D:
         _native.check(_native.lib().qmhd_solver_divergence_b_max(self._h, ctypes.byref(d)))
         return d.value
 
+    def set_owned_window(self, x0: int, x1: int, y0: int, y1: int) -> None:
+        """Restrict dt, retry and preflight reductions to interior cells
+        [x0, x1) x [y0, y1) (a tile of a decomposed domain; the rest is halo)."""
+        _native.check(_native.lib().qmhd_solver_set_owned_window(self._h, int(x0), int(x1),
+                                                                 int(y0), int(y1)))
+
+    def write_halo(self, component: str, values) -> None:
+        """Write a whole component whose values come from the solver's own
+        steps (neighbouring tiles' owned cells); the state stays
+        solver-owned."""
+        a = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1))
+        _native.check(_native.lib().qmhd_solver_write_halo(
+            self._h, component.encode(), a.ctypes.data, a.size))
+
     def divergence_b_relative(self) -> float:
         """Dimensionless solenoidality: max |div B| x dx / max |B_face| over
         the evolved faces, the measure the reference's own example tests

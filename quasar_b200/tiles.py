@@ -1,0 +1,386 @@
+"""One MHD instance decomposed over ranks: 2-D tiles with deep halos (the
+"next" multi-GPU row: the reference's distributed runtime,
+src/distributed/mhd_runtime.cpp, exchanges halos, face records and CT
+tables every stage and reduces dt and the admissible fraction over ranks).
+
+Design.  Rank r of a px x py process grid owns a block of cells and steps a
+local MhdSolver2D over that block plus a halo of `halo` cells on every side
+that is not a physical boundary.  The halo is deep enough for a whole SSP-RK3
+step: each stage's residual at a cell depends on cells at most about 15 away
+(MP7: the normal stencil, the transverse Gauss recovery, the collocated
+field and the corner EMF interpolation), so three stages stay inside 48
+cells and the owned cells come out of the local step bit for bit as in the
+undecomposed run.  What crosses ranks per step:
+
+* dt: every rank's cfl_limit() over its owned cells only (the solver's owned
+  window), reduced with MIN: the same dt as the whole domain's;
+* after the step, the halo: every local position another rank owns is
+  refreshed from that rank (cells and both face fields; a face belongs to
+  the owner of the cell above it, the domain's last face to its last cell),
+  written back with write_halo so that the state stays solver-owned;
+* agreement flags (MAX) around each collective so that a rank that fails
+  (a preflight, a positivity retry) takes every rank down with the same
+  error instead of leaving them waiting in the next collective.
+
+Positivity retries are not coordinated: a step that needs one on any rank
+raises on every rank.  The exchange goes through host buffers and the
+process group (gloo on the host, or NCCL with device tensors); the kernels
+never wait on another rank.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+from . import mhd
+
+CELL = ("rho", "mx", "my", "mz", "energy", "bz_cell")
+COMPONENTS = ("rho", "mx", "my", "mz", "energy", "bx_face", "by_face", "bz_cell")
+DEFAULT_HALO = 48
+
+
+def _split(n: int, parts: int, k: int) -> Tuple[int, int]:
+    return (k * n) // parts, ((k + 1) * n) // parts
+
+
+@dataclasses.dataclass
+class Tile:
+    """Rank `rank`'s piece: owned cells [x0, x1) x [y0, y1) of the global
+    interior and the local domain [lx0, lx0 + nxl) x [ly0, ly0 + nyl) in
+    global cell coordinates (periodic axes may run past the edges)."""
+    rank: int
+    x0: int
+    x1: int
+    y0: int
+    y1: int
+    lx0: int
+    ly0: int
+    nxl: int
+    nyl: int
+    bc: Tuple[str, str, str, str]
+
+    def window(self) -> Tuple[int, int, int, int]:
+        """The owned cells in local interior coordinates."""
+        return (self.x0 - self.lx0, self.x1 - self.lx0, self.y0 - self.ly0, self.y1 - self.ly0)
+
+
+class TileLayout:
+    """px x py decomposition of an nx x ny domain with side boundaries `bc`
+    (x_lo, x_hi, y_lo, y_hi: 'periodic', 'outflow' or 'wall')."""
+
+    def __init__(self, nx: int, ny: int, bc, px: int, py: int, halo: int = DEFAULT_HALO):
+        if px < 1 or py < 1 or px > nx or py > ny:
+            raise ValueError("process grid must be 1 <= px <= nx, 1 <= py <= ny")
+        if (bc[0] == "periodic") != (bc[1] == "periodic") or (bc[2] == "periodic") != (bc[3] == "periodic"):
+            raise ValueError("periodic sides come in pairs")
+        self.nx, self.ny, self.px, self.py, self.halo = nx, ny, px, py, halo
+        self.bc = tuple(bc)
+        self.perx, self.pery = bc[0] == "periodic", bc[2] == "periodic"
+        self.tiles = [self._tile(r) for r in range(px * py)]
+
+    @property
+    def world(self) -> int:
+        return self.px * self.py
+
+    def _axis(self, n, parts, k, periodic, lo_bc, hi_bc):
+        a, b = _split(n, parts, k)
+        if parts == 1:
+            return a, b, 0, n, (lo_bc, hi_bc)
+        if periodic:
+            h = self.halo
+            return a, b, a - h, (b - a) + 2 * h, ("outflow", "outflow")
+        hl, hh = min(self.halo, a), min(self.halo, n - b)
+        return a, b, a - hl, (b - a) + hl + hh, (lo_bc if hl == 0 else "outflow",
+                                                  hi_bc if hh == 0 else "outflow")
+
+    def _tile(self, r: int) -> Tile:
+        rx, ry = r % self.px, r // self.px
+        x0, x1, lx0, nxl, (bxl, bxh) = self._axis(self.nx, self.px, rx, self.perx, self.bc[0], self.bc[1])
+        y0, y1, ly0, nyl, (byl, byh) = self._axis(self.ny, self.py, ry, self.pery, self.bc[2], self.bc[3])
+        return Tile(r, x0, x1, y0, y1, lx0, ly0, nxl, nyl, (bxl, bxh, byl, byh))
+
+    def _owner_x(self, gi: int) -> int:
+        for k in range(self.px):
+            a, b = _split(self.nx, self.px, k)
+            if a <= gi < b:
+                return k
+        raise AssertionError(gi)
+
+    def _owner_y(self, gj: int) -> int:
+        for k in range(self.py):
+            a, b = _split(self.ny, self.py, k)
+            if a <= gj < b:
+                return k
+        raise AssertionError(gj)
+
+    def _global(self, t: Tile, il: int, jl: int, kind: str) -> Tuple[int, int]:
+        """Global position of local interior position (il, jl) of `kind`
+        ('cell', 'xface', 'yface'), wrapped on periodic axes."""
+        gi, gj = il + t.lx0, jl + t.ly0
+        if self.perx:
+            gi %= self.nx
+        if self.pery:
+            gj %= self.ny
+        return gi, gj
+
+    def owner(self, gi: int, gj: int, kind: str) -> int:
+        """Rank owning a global position: a cell's tile; a face, the tile of
+        the cell above it (the domain's last face: its last cell's)."""
+        ci = min(gi, self.nx - 1) if kind == "xface" else gi
+        cj = min(gj, self.ny - 1) if kind == "yface" else gj
+        return self._owner_x(ci) + self.px * self._owner_y(cj)
+
+    def positions(self, t: Tile, kind: str):
+        """Local interior positions of `kind` the local step evolves, row by row."""
+        ni = t.nxl + (1 if kind == "xface" else 0)
+        nj = t.nyl + (1 if kind == "yface" else 0)
+        for jl in range(nj):
+            for il in range(ni):
+                yield il, jl
+
+    def exchange_plan(self, rank: int, ng: int) -> Dict[int, Dict[str, Tuple[np.ndarray, np.ndarray]]]:
+        """For every peer p (this rank included for wrapped copies):
+        plan[p][kind] = (indices into this rank's padded local arrays that
+        receive from p, indices into p's padded local arrays that p sends),
+        in one agreed order (this rank's positions row by row)."""
+        t = self.tiles[rank]
+        pitch = t.nxl + 2 * ng
+        plan: Dict[int, Dict[str, Tuple[list, list]]] = {}
+        for kind in ("cell", "xface", "yface"):
+            for il, jl in self.positions(t, kind):
+                gi, gj = self._global(t, il, jl, kind)
+                p = self.owner(gi, gj, kind)
+                if p == rank and self._owned_here(t, il, jl, kind):
+                    continue
+                src = self.tiles[p]
+                sil, sjl = self._local_of_owner(src, gi, gj, kind)
+                dst_k = (il + ng) + pitch * (jl + ng)
+                src_k = (sil + ng) + (src.nxl + 2 * ng) * (sjl + ng)
+                d = plan.setdefault(p, {}).setdefault(kind, ([], []))
+                d[0].append(dst_k)
+                d[1].append(src_k)
+        return {p: {k: (np.array(a, dtype=np.int64), np.array(b, dtype=np.int64))
+                    for k, (a, b) in v.items()} for p, v in plan.items()}
+
+    def _owned_here(self, t: Tile, il: int, jl: int, kind: str) -> bool:
+        """Whether local position (il, jl) is the owner's own copy (inside
+        the owned block, not a periodic image of it)."""
+        gi, gj = il + t.lx0, jl + t.ly0
+        xi = t.x0 <= gi < t.x1 or (kind == "xface" and gi == t.x1 == self.nx and not self.perx)
+        yj = t.y0 <= gj < t.y1 or (kind == "yface" and gj == t.y1 == self.ny and not self.pery)
+        return xi and yj
+
+    def _local_of_owner(self, src: Tile, gi: int, gj: int, kind: str) -> Tuple[int, int]:
+        """The owner's local coordinates of a global position it owns."""
+        return gi - src.lx0, gj - src.ly0
+
+    def local_grid_config(self, cfg: mhd.MhdConfig, rank: int) -> mhd.MhdConfig:
+        t = self.tiles[rank]
+        g = cfg.grid
+        dx, dy = g.lx / g.nx, g.ly / g.ny
+        c = dataclasses.replace(cfg)
+        c.grid = mhd.Grid2D(t.nxl, t.nyl, t.nxl * dx, t.nyl * dy,
+                            g.origin_x + t.lx0 * dx, g.origin_y + t.ly0 * dy)
+        c.boundary = mhd.MhdBoundarySpec(list(t.bc), list(t.bc))
+        return c
+
+    def kind_of(self, name: str) -> str:
+        return "xface" if name == "bx_face" else "yface" if name == "by_face" else "cell"
+
+
+def extract_local(layout: TileLayout, rank: int, global_padded: np.ndarray, name: str,
+                  ng: int) -> np.ndarray:
+    """This rank's padded local array cut from a global padded array (the
+    global array's ghost layers must hold at least ng cells; periodic axes
+    wrap through the interior)."""
+    t = layout.tiles[rank]
+    gp = global_padded.reshape(layout.ny + 2 * ng, layout.nx + 2 * ng)
+    out = np.zeros((t.nyl + 2 * ng, t.nxl + 2 * ng))
+    for jl in range(-ng, t.nyl + ng):
+        gj = jl + t.ly0
+        if layout.pery:
+            gj %= layout.ny
+        if not -ng <= gj < layout.ny + ng:
+            continue
+        for il in range(-ng, t.nxl + ng):
+            gi = il + t.lx0
+            if layout.perx:
+                gi %= layout.nx
+            if not -ng <= gi < layout.nx + ng:
+                continue
+            out[jl + ng, il + ng] = gp[gj + ng, gi + ng]
+    return out.reshape(-1)
+
+
+class TiledSolver:
+    """The rank's tile of a decomposed MhdSolver2D over a process group
+    (torch.distributed, initialised by the caller).  Every rank calls every
+    method in the same order."""
+
+    def __init__(self, cfg: mhd.MhdConfig, px: int, py: int, halo: int = DEFAULT_HALO,
+                 group=None, device: str = "cpu"):
+        import torch.distributed as dist
+        self.dist, self.group, self.device = dist, group, device
+        self.rank = dist.get_rank(group)
+        world = dist.get_world_size(group)
+        g = cfg.grid
+        side = list(cfg.boundary.fluid)
+        self.layout = TileLayout(g.nx, g.ny, side, px, py, halo)
+        if self.layout.world != world:
+            raise ValueError(f"process grid {px}x{py} needs {px * py} ranks, the group has {world}")
+        self.cfg = cfg
+        self.local = mhd.MhdSolver2D(self.layout.local_grid_config(cfg, self.rank))
+        self.ng = self.local.grid().nghost
+        self.tile = self.layout.tiles[self.rank]
+        self.local.set_owned_window(*self.tile.window())
+        self.plans = [self.layout.exchange_plan(r, self.ng) for r in range(world)]
+
+    # ---- agreement and reductions -------------------------------------------
+    def _reduce(self, value: float, op: str) -> float:
+        import torch
+        t = torch.tensor([float(value)], dtype=torch.float64, device=self.device)
+        o = self.dist.ReduceOp.MIN if op == "min" else self.dist.ReduceOp.MAX if op == "max" else \
+            self.dist.ReduceOp.SUM
+        self.dist.all_reduce(t, op=o, group=self.group)
+        return float(t.item())
+
+    def _agree(self, fn):
+        """Run fn on every rank; if it raised anywhere, raise everywhere."""
+        err, out = None, None
+        try:
+            out = fn()
+        except (RuntimeError, ValueError) as e:
+            err = e
+        if self._reduce(1.0 if err else 0.0, "max") > 0.0:
+            raise err if err else RuntimeError("tiled solver: another rank failed")
+        return out
+
+    # ---- seeding and stepping ------------------------------------------------
+    def seed_global(self, name: str, global_padded) -> None:
+        """Seed component `name` from the whole domain's padded array (every
+        rank passes the same array)."""
+        arr = extract_local(self.layout, self.rank, np.asarray(global_padded, dtype=np.float64),
+                            name, self.ng)
+        self._agree(lambda: self.local.seed_state(name, arr))
+
+    def cfl_limit(self) -> float:
+        dt = self._agree(self.local.cfl_limit)
+        return self._reduce(dt, "min")
+
+    def step_unchecked(self, dt: float) -> None:
+        def run():
+            self.local.step_unchecked(dt)
+            if self.local.last_positivity_substeps() > 1:
+                raise RuntimeError("tiled solver: a positivity retry is not coordinated across "
+                                   "tiles; step the undecomposed solver")
+        self._agree(run)
+        self.exchange()
+
+    def advance_steps(self, steps: int) -> float:
+        t = 0.0
+        for _ in range(steps):
+            dt = self.cfl_limit()
+            self.step_unchecked(dt)
+            t += dt
+        return t
+
+    # ---- halo exchange ------------------------------------------------------
+    def exchange(self) -> None:
+        """Refresh every local position another rank owns from that rank."""
+        import torch
+        arrays = {n: self.local.state_component_to_host(n) for n in COMPONENTS}
+        world = self.layout.world
+        kinds = {n: self.layout.kind_of(n) for n in COMPONENTS}
+        sends, recvs = {}, {}
+        for p in range(world):
+            # what p needs from me, in p's order
+            need = self.plans[p].get(self.rank, {})
+            parts = [arrays[n][need[kinds[n]][1]] for n in COMPONENTS if kinds[n] in need]
+            if p == self.rank:
+                continue
+            if parts:
+                buf = torch.from_numpy(np.concatenate(parts)).to(self.device)
+                sends[p] = buf
+        mine = self.plans[self.rank]
+        for p in range(world):
+            if p == self.rank or p not in mine:
+                continue
+            size = sum(len(mine[p][kinds[n]][0]) for n in COMPONENTS if kinds[n] in mine[p])
+            recvs[p] = torch.empty(size, dtype=torch.float64, device=self.device)
+        # pairwise in rank order: lower rank sends first, so gloo never deadlocks
+        for p in sorted(set(sends) | set(recvs)):
+            if self.rank < p:
+                if p in sends:
+                    self.dist.send(sends[p], dst=p, group=self.group)
+                if p in recvs:
+                    self.dist.recv(recvs[p], src=p, group=self.group)
+            else:
+                if p in recvs:
+                    self.dist.recv(recvs[p], src=p, group=self.group)
+                if p in sends:
+                    self.dist.send(sends[p], dst=p, group=self.group)
+        for p, buf in recvs.items():
+            data, off = buf.cpu().numpy(), 0
+            for n in COMPONENTS:
+                k = kinds[n]
+                if k not in mine[p]:
+                    continue
+                dst = mine[p][k][0]
+                arrays[n][dst] = data[off:off + len(dst)]
+                off += len(dst)
+        if self.rank in mine:  # periodic images of this rank's own cells
+            for n in COMPONENTS:
+                k = kinds[n]
+                if k in mine[self.rank]:
+                    dst, src = mine[self.rank][k]
+                    arrays[n][dst] = arrays[n][src]
+        self._agree(lambda: [self.local.write_halo(n, arrays[n]) for n in COMPONENTS])
+
+    # ---- gathering -----------------------------------------------------------
+    def owned_block(self, name: str) -> np.ndarray:
+        """This rank's owned values of `name` in local storage order
+        (cells, or the faces the rank owns)."""
+        return self.local.state_component_to_host(name)
+
+    def gather(self, name: str) -> np.ndarray:
+        """The whole domain's padded array of `name` on every rank (interior
+        cells and evolved faces filled from their owners; ghosts zero)."""
+        import torch
+        ng, lay = self.ng, self.layout
+        kind = lay.kind_of(name)
+        pitch = lay.nx + 2 * ng
+        local = self.local.state_component_to_host(name)
+        t = self.tile
+        lp = t.nxl + 2 * ng
+        gidx, vals = [], []
+        for il, jl in lay.positions(t, kind):
+            gi, gj = lay._global(t, il, jl, kind)
+            if lay.owner(gi, gj, kind) == self.rank and lay._owned_here(t, il, jl, kind):
+                gidx.append((gi + ng) + pitch * (gj + ng))
+                vals.append(local[(il + ng) + lp * (jl + ng)])
+        n = torch.tensor([len(gidx)], dtype=torch.int64)
+        sizes = [torch.zeros(1, dtype=torch.int64) for _ in range(lay.world)]
+        self.dist.all_gather(sizes, n, group=self.group)
+        m = int(max(s.item() for s in sizes))
+        gi_t = torch.full((m,), -1, dtype=torch.int64)
+        gi_t[:len(gidx)] = torch.tensor(gidx, dtype=torch.int64)
+        v_t = torch.zeros(m, dtype=torch.float64)
+        v_t[:len(vals)] = torch.tensor(vals, dtype=torch.float64)
+        all_i = [torch.empty(m, dtype=torch.int64) for _ in range(lay.world)]
+        all_v = [torch.empty(m, dtype=torch.float64) for _ in range(lay.world)]
+        self.dist.all_gather(all_i, gi_t, group=self.group)
+        self.dist.all_gather(all_v, v_t, group=self.group)
+        out = np.zeros((lay.ny + 2 * ng) * pitch)
+        for a, b in zip(all_i, all_v):
+            a, b = a.numpy(), b.numpy()
+            keep = a >= 0
+            out[a[keep]] = b[keep]
+        # a periodic axis's last face is the image of its first
+        o = out.reshape(lay.ny + 2 * ng, pitch)
+        if kind == "xface" and lay.perx:
+            o[ng:ng + lay.ny, ng + lay.nx] = o[ng:ng + lay.ny, ng]
+        if kind == "yface" and lay.pery:
+            o[ng + lay.ny, ng:ng + lay.nx] = o[ng, ng:ng + lay.nx]
+        return out

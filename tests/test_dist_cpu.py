@@ -5,6 +5,7 @@ import os
 import socket
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -118,3 +119,97 @@ def test_partition_rules():
     assert shard.imbalance([1] * 8, 4) == 1.0
     with pytest.raises(ValueError):
         shard.partition([1], 0)
+
+
+class _ArraySolver:
+    """Stand-in for a tile's local solver on the CPU: numpy arrays behind
+    state_component_to_host / write_halo."""
+
+    def __init__(self, arrays):
+        self.arrays = arrays
+
+    def state_component_to_host(self, name):
+        return self.arrays[name].copy()
+
+    def write_halo(self, name, values):
+        self.arrays[name] = np.asarray(values, dtype=np.float64).copy()
+
+
+def _tile_rank(rank, world, port, q, nx, ny, bc, px, py, halo):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import torch.distributed as dist
+
+    from quasar_b200 import tiles
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    ng = 3
+    lay = tiles.TileLayout(nx, ny, bc, px, py, halo)
+    rng = np.random.default_rng(7)
+    glob = {n: rng.standard_normal((ny + 2 * ng) * (nx + 2 * ng)) for n in tiles.COMPONENTS}
+    t = lay.tiles[rank]
+    loc = {n: tiles.extract_local(lay, rank, glob[n], n, ng) for n in tiles.COMPONENTS}
+    want = {n: a.copy() for n, a in loc.items()}
+    # every position this tile does not own is stale before the exchange
+    lp = t.nxl + 2 * ng
+    for n in tiles.COMPONENTS:
+        kind = lay.kind_of(n)
+        for il, jl in lay.positions(t, kind):
+            gi, gj = lay._global(t, il, jl, kind)
+            if not (lay.owner(gi, gj, kind) == rank and lay._owned_here(t, il, jl, kind)):
+                loc[n][(il + ng) + lp * (jl + ng)] = np.nan
+    ts = tiles.TiledSolver.__new__(tiles.TiledSolver)
+    ts.dist, ts.group, ts.device, ts.rank = dist, None, "cpu", rank
+    ts.layout, ts.tile, ts.ng = lay, t, ng
+    ts.local = _ArraySolver(loc)
+    ts.plans = [lay.exchange_plan(r, ng) for r in range(world)]
+    ts.exchange()
+    ok = True
+    for n in tiles.COMPONENTS:
+        kind = lay.kind_of(n)
+        for il, jl in lay.positions(t, kind):
+            k = (il + ng) + lp * (jl + ng)
+            ok = ok and ts.local.arrays[n][k] == want[n][k]
+    g = {n: ts.gather(n) for n in ("rho", "bx_face", "by_face")}
+    pitch = nx + 2 * ng
+    gat = True
+    for n, kind in (("rho", "cell"), ("bx_face", "xface"), ("by_face", "yface")):
+        gp, ref = g[n].reshape(-1, pitch), glob[n].reshape(-1, pitch)
+        ni, nj = nx + (kind == "xface"), ny + (kind == "yface")
+        sub, rsub = gp[ng:ng + nj, ng:ng + ni], ref[ng:ng + nj, ng:ng + ni]
+        if kind == "xface" and bc[0] == "periodic":
+            sub, rsub = sub[:, :nx], rsub[:, :nx]
+        if kind == "yface" and bc[2] == "periodic":
+            sub, rsub = sub[:ny], rsub[:ny]
+        gat = gat and np.array_equal(sub, rsub)
+    dist.destroy_process_group()
+    q.put((rank, bool(ok), bool(gat)))
+
+
+@pytest.mark.parametrize("nx,ny,bc,px,py,halo", [
+    (24, 20, ("periodic",) * 4, 2, 1, 6),
+    (24, 20, ("outflow",) * 4, 1, 2, 5),
+    (17, 13, ("periodic", "periodic", "outflow", "outflow"), 2, 2, 4),
+    (10, 12, ("periodic",) * 4, 2, 2, 7),   # halos wider than a tile: periodic images
+])
+def test_tile_halo_exchange_over_gloo(nx, ny, bc, px, py, halo):
+    """The tile runtime's exchange (quasar_b200/tiles.py) on gloo ranks with
+    numpy arrays in place of the solvers: every position a tile does not own
+    (cells and both face fields, periodic images included) comes back equal
+    to the whole domain's value, and gathering the owned values rebuilds the
+    whole domain."""
+    import torch.multiprocessing as mp
+    world = px * py
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_tile_rank, args=(r, world, port, q, nx, ny, bc, px, py, halo))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(ok and gat for _, ok, gat in out), out
