@@ -34,6 +34,13 @@ __device__ __forceinline__ float gelu(float x) {
   return 0.5f * x * (1.0f + t);
 }
 
+// Two floats rounded to BF16 (nearest even) in one conversion, the first in
+// the low half: the packing of consecutive K-major operand columns.
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
 __device__ __forceinline__ uint16_t to_bf16(float x) {
   return __bfloat16_as_ushort(__float2bfloat16_rn(x));
 }
@@ -201,10 +208,10 @@ __device__ __forceinline__ uint4 features8(const float* q, const float* c, const
   f[6] = clampf((q[6] - c[6]) * n.isb);
   f[7] = clampf((q[7] - c[7]) * n.isb);
   uint4 r;
-  r.x = uint32_t(to_bf16(f[0])) | (uint32_t(to_bf16(f[1])) << 16);
-  r.y = uint32_t(to_bf16(f[2])) | (uint32_t(to_bf16(f[3])) << 16);
-  r.z = uint32_t(to_bf16(f[4])) | (uint32_t(to_bf16(f[5])) << 16);
-  r.w = uint32_t(to_bf16(f[6])) | (uint32_t(to_bf16(f[7])) << 16);
+  r.x = pack_bf16x2(f[0], f[1]);
+  r.y = pack_bf16x2(f[2], f[3]);
+  r.z = pack_bf16x2(f[4], f[5]);
+  r.w = pack_bf16x2(f[6], f[7]);
   return r;
 }
 
@@ -651,8 +658,8 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
         uint32_t w[4];
 #pragma unroll
         for (int c = 0; c < 8; c += 2)
-          w[c / 2] = uint32_t(to_bf16(gelu(z[h + c] + p.b1[c0 + h + c]))) |
-                     (uint32_t(to_bf16(gelu(z[h + c + 1] + p.b1[c0 + h + c + 1]))) << 16);
+          w[c / 2] = pack_bf16x2(gelu(z[h + c] + p.b1[c0 + h + c]),
+                                 gelu(z[h + c + 1] + p.b1[c0 + h + c + 1]));
         *reinterpret_cast<uint4*>(a1s + tc::kmajor_offset(row, c0 + h, kHidden)) =
             make_uint4(w[0], w[1], w[2], w[3]);
       }

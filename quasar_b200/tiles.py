@@ -30,7 +30,7 @@ never wait on another rank.
 from __future__ import annotations
 
 import dataclasses
-from typing import Dict, List, Tuple
+from typing import Dict, Tuple
 
 import numpy as np
 
@@ -101,44 +101,50 @@ class TileLayout:
         y0, y1, ly0, nyl, (byl, byh) = self._axis(self.ny, self.py, ry, self.pery, self.bc[2], self.bc[3])
         return Tile(r, x0, x1, y0, y1, lx0, ly0, nxl, nyl, (bxl, bxh, byl, byh))
 
-    def _owner_x(self, gi: int) -> int:
-        for k in range(self.px):
-            a, b = _split(self.nx, self.px, k)
-            if a <= gi < b:
-                return k
-        raise AssertionError(gi)
+    def _bounds(self, n: int, parts: int) -> np.ndarray:
+        return np.array([(k * n) // parts for k in range(parts + 1)])
 
-    def _owner_y(self, gj: int) -> int:
-        for k in range(self.py):
-            a, b = _split(self.ny, self.py, k)
-            if a <= gj < b:
-                return k
-        raise AssertionError(gj)
-
-    def _global(self, t: Tile, il: int, jl: int, kind: str) -> Tuple[int, int]:
-        """Global position of local interior position (il, jl) of `kind`
-        ('cell', 'xface', 'yface'), wrapped on periodic axes."""
-        gi, gj = il + t.lx0, jl + t.ly0
-        if self.perx:
-            gi %= self.nx
-        if self.pery:
-            gj %= self.ny
-        return gi, gj
-
-    def owner(self, gi: int, gj: int, kind: str) -> int:
-        """Rank owning a global position: a cell's tile; a face, the tile of
-        the cell above it (the domain's last face: its last cell's)."""
-        ci = min(gi, self.nx - 1) if kind == "xface" else gi
-        cj = min(gj, self.ny - 1) if kind == "yface" else gj
-        return self._owner_x(ci) + self.px * self._owner_y(cj)
+    def owner(self, gi, gj, kind: str):
+        """Rank owning global positions (arrays or scalars): a cell's tile; a
+        face, the tile of the cell above it (the domain's last face: its
+        last cell's)."""
+        gi, gj = np.asarray(gi), np.asarray(gj)
+        ci = np.minimum(gi, self.nx - 1) if kind == "xface" else gi
+        cj = np.minimum(gj, self.ny - 1) if kind == "yface" else gj
+        ox = np.searchsorted(self._bounds(self.nx, self.px), ci, side="right") - 1
+        oy = np.searchsorted(self._bounds(self.ny, self.py), cj, side="right") - 1
+        r = ox + self.px * oy
+        return int(r) if r.ndim == 0 else r
 
     def positions(self, t: Tile, kind: str):
-        """Local interior positions of `kind` the local step evolves, row by row."""
+        """Local interior positions (il, jl) of `kind` the local step evolves,
+        row by row, as two index arrays."""
         ni = t.nxl + (1 if kind == "xface" else 0)
         nj = t.nyl + (1 if kind == "yface" else 0)
-        for jl in range(nj):
-            for il in range(ni):
-                yield il, jl
+        jl, il = np.meshgrid(np.arange(nj), np.arange(ni), indexing="ij")
+        return il.ravel(), jl.ravel()
+
+    def _global(self, t: Tile, il, jl, kind: str):
+        """Global positions of local interior positions of `kind` ('cell',
+        'xface', 'yface'), wrapped on periodic axes."""
+        gi, gj = np.asarray(il) + t.lx0, np.asarray(jl) + t.ly0
+        if self.perx:
+            gi = gi % self.nx
+        if self.pery:
+            gj = gj % self.ny
+        return gi, gj
+
+    def _owned_here(self, t: Tile, il, jl, kind: str):
+        """Whether local positions are the owner's own copy (inside the owned
+        block, not a periodic image of it)."""
+        gi, gj = np.asarray(il) + t.lx0, np.asarray(jl) + t.ly0
+        xi = (t.x0 <= gi) & (gi < t.x1)
+        yj = (t.y0 <= gj) & (gj < t.y1)
+        if kind == "xface" and not self.perx and t.x1 == self.nx:
+            xi = xi | (gi == self.nx)
+        if kind == "yface" and not self.pery and t.y1 == self.ny:
+            yj = yj | (gj == self.ny)
+        return xi & yj
 
     def exchange_plan(self, rank: int, ng: int) -> Dict[int, Dict[str, Tuple[np.ndarray, np.ndarray]]]:
         """For every peer p (this rank included for wrapped copies):
@@ -147,34 +153,22 @@ class TileLayout:
         in one agreed order (this rank's positions row by row)."""
         t = self.tiles[rank]
         pitch = t.nxl + 2 * ng
-        plan: Dict[int, Dict[str, Tuple[list, list]]] = {}
+        plan: Dict[int, Dict[str, Tuple[np.ndarray, np.ndarray]]] = {}
         for kind in ("cell", "xface", "yface"):
-            for il, jl in self.positions(t, kind):
-                gi, gj = self._global(t, il, jl, kind)
-                p = self.owner(gi, gj, kind)
-                if p == rank and self._owned_here(t, il, jl, kind):
-                    continue
-                src = self.tiles[p]
-                sil, sjl = self._local_of_owner(src, gi, gj, kind)
-                dst_k = (il + ng) + pitch * (jl + ng)
-                src_k = (sil + ng) + (src.nxl + 2 * ng) * (sjl + ng)
-                d = plan.setdefault(p, {}).setdefault(kind, ([], []))
-                d[0].append(dst_k)
-                d[1].append(src_k)
-        return {p: {k: (np.array(a, dtype=np.int64), np.array(b, dtype=np.int64))
-                    for k, (a, b) in v.items()} for p, v in plan.items()}
-
-    def _owned_here(self, t: Tile, il: int, jl: int, kind: str) -> bool:
-        """Whether local position (il, jl) is the owner's own copy (inside
-        the owned block, not a periodic image of it)."""
-        gi, gj = il + t.lx0, jl + t.ly0
-        xi = t.x0 <= gi < t.x1 or (kind == "xface" and gi == t.x1 == self.nx and not self.perx)
-        yj = t.y0 <= gj < t.y1 or (kind == "yface" and gj == t.y1 == self.ny and not self.pery)
-        return xi and yj
-
-    def _local_of_owner(self, src: Tile, gi: int, gj: int, kind: str) -> Tuple[int, int]:
-        """The owner's local coordinates of a global position it owns."""
-        return gi - src.lx0, gj - src.ly0
+            il, jl = self.positions(t, kind)
+            gi, gj = self._global(t, il, jl, kind)
+            own = self.owner(gi, gj, kind)
+            take = ~((own == rank) & self._owned_here(t, il, jl, kind))
+            il, jl, gi, gj, own = il[take], jl[take], gi[take], gj[take], own[take]
+            dst_all = (il + ng) + pitch * (jl + ng)
+            for p in np.unique(own):
+                sel = own == p
+                src = self.tiles[int(p)]
+                # the owner's local coordinates of the positions it owns
+                src_k = (gi[sel] - src.lx0 + ng) + (src.nxl + 2 * ng) * (gj[sel] - src.ly0 + ng)
+                plan.setdefault(int(p), {})[kind] = (dst_all[sel].astype(np.int64),
+                                                     src_k.astype(np.int64))
+        return plan
 
     def local_grid_config(self, cfg: mhd.MhdConfig, rank: int) -> mhd.MhdConfig:
         t = self.tiles[rank]
@@ -196,21 +190,17 @@ def extract_local(layout: TileLayout, rank: int, global_padded: np.ndarray, name
     global array's ghost layers must hold at least ng cells; periodic axes
     wrap through the interior)."""
     t = layout.tiles[rank]
-    gp = global_padded.reshape(layout.ny + 2 * ng, layout.nx + 2 * ng)
+    gp = np.asarray(global_padded).reshape(layout.ny + 2 * ng, layout.nx + 2 * ng)
+    gi = np.arange(-ng, t.nxl + ng) + t.lx0
+    gj = np.arange(-ng, t.nyl + ng) + t.ly0
+    if layout.perx:
+        gi = gi % layout.nx
+    if layout.pery:
+        gj = gj % layout.ny
+    okx = (gi >= -ng) & (gi < layout.nx + ng)
+    oky = (gj >= -ng) & (gj < layout.ny + ng)
     out = np.zeros((t.nyl + 2 * ng, t.nxl + 2 * ng))
-    for jl in range(-ng, t.nyl + ng):
-        gj = jl + t.ly0
-        if layout.pery:
-            gj %= layout.ny
-        if not -ng <= gj < layout.ny + ng:
-            continue
-        for il in range(-ng, t.nxl + ng):
-            gi = il + t.lx0
-            if layout.perx:
-                gi %= layout.nx
-            if not -ng <= gi < layout.nx + ng:
-                continue
-            out[jl + ng, il + ng] = gp[gj + ng, gi + ng]
+    out[np.ix_(oky, okx)] = gp[np.ix_(gj[oky] + ng, gi[okx] + ng)]
     return out.reshape(-1)
 
 
@@ -354,12 +344,11 @@ class TiledSolver:
         local = self.local.state_component_to_host(name)
         t = self.tile
         lp = t.nxl + 2 * ng
-        gidx, vals = [], []
-        for il, jl in lay.positions(t, kind):
-            gi, gj = lay._global(t, il, jl, kind)
-            if lay.owner(gi, gj, kind) == self.rank and lay._owned_here(t, il, jl, kind):
-                gidx.append((gi + ng) + pitch * (gj + ng))
-                vals.append(local[(il + ng) + lp * (jl + ng)])
+        il, jl = lay.positions(t, kind)
+        gi, gj = lay._global(t, il, jl, kind)
+        mine = (lay.owner(gi, gj, kind) == self.rank) & lay._owned_here(t, il, jl, kind)
+        gidx = ((gi[mine] + ng) + pitch * (gj[mine] + ng)).tolist()
+        vals = local[(il[mine] + ng) + lp * (jl[mine] + ng)].tolist()
         n = torch.tensor([len(gidx)], dtype=torch.int64)
         sizes = [torch.zeros(1, dtype=torch.int64) for _ in range(lay.world)]
         self.dist.all_gather(sizes, n, group=self.group)

@@ -155,10 +155,10 @@ def _tile_rank(rank, world, port, q, nx, ny, bc, px, py, halo):
     lp = t.nxl + 2 * ng
     for n in tiles.COMPONENTS:
         kind = lay.kind_of(n)
-        for il, jl in lay.positions(t, kind):
-            gi, gj = lay._global(t, il, jl, kind)
-            if not (lay.owner(gi, gj, kind) == rank and lay._owned_here(t, il, jl, kind)):
-                loc[n][(il + ng) + lp * (jl + ng)] = np.nan
+        il, jl = lay.positions(t, kind)
+        gi, gj = lay._global(t, il, jl, kind)
+        stale = ~((lay.owner(gi, gj, kind) == rank) & lay._owned_here(t, il, jl, kind))
+        loc[n][(il[stale] + ng) + lp * (jl[stale] + ng)] = np.nan
     ts = tiles.TiledSolver.__new__(tiles.TiledSolver)
     ts.dist, ts.group, ts.device, ts.rank = dist, None, "cpu", rank
     ts.layout, ts.tile, ts.ng = lay, t, ng
@@ -167,10 +167,9 @@ def _tile_rank(rank, world, port, q, nx, ny, bc, px, py, halo):
     ts.exchange()
     ok = True
     for n in tiles.COMPONENTS:
-        kind = lay.kind_of(n)
-        for il, jl in lay.positions(t, kind):
-            k = (il + ng) + lp * (jl + ng)
-            ok = ok and ts.local.arrays[n][k] == want[n][k]
+        il, jl = lay.positions(t, lay.kind_of(n))
+        k = (il + ng) + lp * (jl + ng)
+        ok = ok and np.array_equal(ts.local.arrays[n][k], want[n][k])
     g = {n: ts.gather(n) for n in ("rho", "bx_face", "by_face")}
     pitch = nx + 2 * ng
     gat = True
