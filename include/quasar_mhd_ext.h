@@ -48,6 +48,27 @@ int qmhd_solver_set_owned_window(qmhd_solver* solver, int x0, int x1, int y0, in
 int qmhd_solver_write_halo(qmhd_solver* solver, const char* component, const double* values,
                            size_t n);
 
+/* The halo exchange without the host round trip of whole components:
+ *
+ * qmhd_solver_gather_live: out[k] = live value of `component` at storage
+ * index idx[k] (row-major padded storage, 0 <= idx[k] < storage size), for
+ * k < n: what this tile sends to a neighbour.
+ *
+ * qmhd_solver_scatter_halo: live value at idx[k] = values[k], for k < n:
+ * what this tile receives.  The values must be finite and come from the
+ * solver's own steps (as for qmhd_solver_write_halo, the state stays
+ * solver-owned); on a bad index or a non-finite value nothing is written
+ * and the call fails with QMHD_INVALID_ARGUMENT.
+ *
+ * idx, out and values are DEVICE memory of the solver's device, each
+ * inside one allocation (checked), and must be ready when the call is made
+ * (their producer's stream synchronised).  Both calls return once the copy
+ * finished. */
+int qmhd_solver_gather_live(qmhd_solver* solver, const char* component, const long long* idx,
+                            size_t n, double* out);
+int qmhd_solver_scatter_halo(qmhd_solver* solver, const char* component, const long long* idx,
+                             size_t n, const double* values);
+
 /* Largest nx*ny accepted by qmhd_conserved_cell_totals_device. */
 #define QMHD_TOTALS_DEVICE_MAX_CELLS 67108864LL
 

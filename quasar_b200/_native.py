@@ -25,7 +25,7 @@ EXPORTS = (
 )
 EXT_EXPORTS = ("qmhd_solver_time_auto_steps", "qmhd_solver_profile_step", "qmhd_fp64_fma_peak",
                "qmhd_conserved_cell_totals_device", "qmhd_solver_set_owned_window",
-               "qmhd_solver_write_halo")
+               "qmhd_solver_write_halo", "qmhd_solver_gather_live", "qmhd_solver_scatter_halo")
 TOTALS_DEVICE_MAX_CELLS = 67108864
 BATCH_EXPORTS = ("qmhd_batch_create", "qmhd_batch_destroy", "qmhd_batch_size", "qmhd_batch_zones",
                  "qmhd_batch_instance", "qmhd_batch_advance", "qmhd_batch_time_steps",
@@ -92,6 +92,8 @@ def lib() -> ctypes.CDLL:
     L.qmhd_solver_advance_auto.argtypes = [vp, dp, ctypes.c_double, ctypes.c_int, ip]
     L.qmhd_solver_set_owned_window.argtypes = [vp] + [ctypes.c_int] * 4
     L.qmhd_solver_write_halo.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_size_t]
+    L.qmhd_solver_gather_live.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_size_t, vp]
+    L.qmhd_solver_scatter_halo.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_size_t, vp]
     L.qmhd_solver_time_auto_steps.argtypes = [vp, ctypes.c_int, dp, ip]
     L.qmhd_solver_profile_step.argtypes = [vp, dp, ctypes.c_int]
     L.qmhd_fp64_fma_peak.argtypes = [dp]

@@ -167,6 +167,30 @@ int qmhd_solver_write_halo(qmhd_solver* s, const char* component, const double* 
   });
 }
 
+int qmhd_solver_gather_live(qmhd_solver* s, const char* component, const long long* idx,
+                            size_t n, double* out) {
+  return guarded([&] {
+    need(s);
+    if (n > 0) {
+      need(idx);
+      need(out);
+    }
+    s->impl->gather_live(component_index(component, false), idx, (long long)n, out);
+  });
+}
+
+int qmhd_solver_scatter_halo(qmhd_solver* s, const char* component, const long long* idx,
+                             size_t n, const double* values) {
+  return guarded([&] {
+    need(s);
+    if (n > 0) {
+      need(idx);
+      need(values);
+    }
+    s->impl->scatter_halo(component_index(component, false), idx, (long long)n, values);
+  });
+}
+
 int qmhd_solver_state_component_to_host(qmhd_solver* s, const char* component, double* out,
                                         size_t n) {
   return guarded([&] {

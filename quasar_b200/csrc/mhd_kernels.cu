@@ -2790,6 +2790,68 @@ void launch_cell_sums(const Grid& g, const StateP& u, double* partial, int block
   k_cell_sums<<<blocks, 256, 0, s>>>(g, u, partial);
 }
 
+// ---- tile halo exchange on the device ---------------------------------------
+// Gather and scatter one component by storage index.  Bad indices and
+// non-finite values are recorded in *bad (bit 0: index outside [0, size),
+// bit 1: non-finite value); the scatter runs as a check pass and a write
+// pass, and the write pass does nothing once the check recorded a problem,
+// so a rejected scatter leaves the component untouched.
+__global__ void k_gather_values(const double* __restrict__ src, const long long* __restrict__ idx,
+                                long long n, long long size, double* __restrict__ out,
+                                unsigned long long* bad) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += stride) {
+    const long long i = idx[k];
+    if (i < 0 || i >= size) {
+      atomicOr(bad, 1ull);
+      out[k] = 0.0;
+    } else {
+      out[k] = src[i];
+    }
+  }
+}
+
+__global__ void k_scatter_check(const long long* __restrict__ idx, const double* __restrict__ v,
+                                long long n, long long size, unsigned long long* bad) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  unsigned long long b = 0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += stride) {
+    const long long i = idx[k];
+    if (i < 0 || i >= size) b |= 1ull;
+    if (!isfinite(v[k])) b |= 2ull;
+  }
+  if (b) atomicOr(bad, b);
+}
+
+__global__ void k_scatter_values(double* __restrict__ dst, const long long* __restrict__ idx,
+                                 const double* __restrict__ v, long long n,
+                                 const unsigned long long* bad) {
+  if (*bad) return;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += stride)
+    dst[idx[k]] = v[k];
+}
+
+namespace {
+int exchange_blocks(long long n) {
+  const long long b = (n + 255) / 256;
+  return (int)(b < 4 * 148 ? (b > 0 ? b : 1) : 4 * 148);
+}
+}  // namespace
+
+void launch_gather_values(const double* src, const long long* idx, long long n, long long size,
+                          double* out, unsigned long long* bad, cudaStream_t s) {
+  if (n <= 0) return;
+  k_gather_values<<<exchange_blocks(n), 256, 0, s>>>(src, idx, n, size, out, bad);
+}
+
+void launch_scatter_values(double* dst, const long long* idx, const double* v, long long n,
+                           long long size, unsigned long long* bad, cudaStream_t s) {
+  if (n <= 0) return;
+  k_scatter_check<<<exchange_blocks(n), 256, 0, s>>>(idx, v, n, size, bad);
+  k_scatter_values<<<exchange_blocks(n), 256, 0, s>>>(dst, idx, v, n, bad);
+}
+
 // ---- batched launchers -----------------------------------------------------
 namespace {
 template <class K>

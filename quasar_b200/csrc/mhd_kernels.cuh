@@ -310,4 +310,14 @@ void launch_reconstruct_learned(const StageArgs& a, int dir, const unsigned char
 void launch_face_lists(const Grid& g, const unsigned char* flag, int* xlist, int* ylist,
                        int* counts, cudaStream_t s);
 
+// ---- tile halo exchange ----------------------------------------------------
+// out[k] = src[idx[k]] and dst[idx[k]] = v[k] for k < n, indices checked
+// against [0, size) and scattered values against non-finite ones; problems
+// are OR-ed into *bad (1: index, 2: value) and a scatter with any problem
+// writes nothing.  *bad must start at zero.
+void launch_gather_values(const double* src, const long long* idx, long long n, long long size,
+                          double* out, unsigned long long* bad, cudaStream_t s);
+void launch_scatter_values(double* dst, const long long* idx, const double* v, long long n,
+                           long long size, unsigned long long* bad, cudaStream_t s);
+
 }  // namespace qb

@@ -5,10 +5,13 @@
 #include "mhd_solver.cuh"
 #include "indicator.cuh"
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <sstream>
 #include <vector>
 
@@ -27,6 +30,37 @@ double from_bits(unsigned long long b) {
 }
 
 int ghosts_for(int order) { return order == 7 ? 4 : order == 5 ? 3 : 2; }
+
+// [p, p + bytes) must lie in one device allocation of `device` (the kernels
+// that read or write it have no other way to know its extent).
+void check_device_range(const void* p, size_t bytes, int device, const char* what) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess ||
+      !(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) ||
+      a.device != device) {
+    cudaGetLastError();
+    throw std::invalid_argument(std::string(what) + " is not device memory of the solver's device");
+  }
+  using RangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+  static RangeFn range = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      range = reinterpret_cast<RangeFn>(fn);
+  });
+  if (!range) throw CudaError("cuMemGetAddressRange is unavailable");
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  if (range(&base, &size, reinterpret_cast<CUdeviceptr>(p)) != CUDA_SUCCESS)
+    throw std::invalid_argument(std::string(what) + ": no device allocation holds it");
+  const CUdeviceptr q = reinterpret_cast<CUdeviceptr>(p);
+  if (q - base > size || bytes > size - (q - base))
+    throw std::invalid_argument(std::string(what) + " runs past the end of its allocation");
+}
 
 }  // namespace
 
@@ -60,6 +94,7 @@ MhdSolver2D::MhdSolver2D(const Config& c) : cfg_(c) {
   g_.dy = c.ly / c.ny;
   for (int s = 0; s < 4; ++s) g_.bc[s] = c.bc[s];
 
+  ck(cudaGetDevice(&device_), "device");
   ck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
   const long long n = g_.size();
   constexpr int kArrays = 5 * 10 + 32 + 16 + 6;
@@ -204,6 +239,41 @@ void MhdSolver2D::write_halo(int comp, const double* host, long long n) {
                      stream_),
      "halo copy");
   ck(cudaStreamSynchronize(stream_), "halo");
+  if (!seeded_dirty_) halo_write_ = solver_owned_;
+  seeded_dirty_ = true;
+  front_order_ = 0;
+}
+
+void MhdSolver2D::gather_live(int comp, const long long* idx, long long n, double* out) {
+  if (comp < 0 || comp > 7) throw std::invalid_argument("MhdSolver2D: unknown state component");
+  if (n < 0) throw std::invalid_argument("MhdSolver2D::gather_live: negative count");
+  if (n == 0) return;
+  check_device_range(idx, sizeof(long long) * n, device_, "gather_live: index buffer");
+  check_device_range(out, sizeof(double) * n, device_, "gather_live: output buffer");
+  ck(cudaMemsetAsync(scalar_, 0, sizeof(unsigned long long), stream_), "memset");
+  launch_gather_values(st_[live_].c[comp], idx, n, g_.size(), out, scalar_, stream_);
+  check_cuda("gather launch");
+  unsigned long long bad = 0;
+  ck(cudaMemcpyAsync(&bad, scalar_, sizeof bad, cudaMemcpyDeviceToHost, stream_), "gather flag");
+  ck(cudaStreamSynchronize(stream_), "gather");
+  if (bad) throw std::invalid_argument("MhdSolver2D::gather_live: storage index out of range");
+}
+
+void MhdSolver2D::scatter_halo(int comp, const long long* idx, long long n, const double* v) {
+  if (comp < 0 || comp > 7) throw std::invalid_argument("MhdSolver2D: unknown state component");
+  if (n < 0) throw std::invalid_argument("MhdSolver2D::scatter_halo: negative count");
+  if (n == 0) return;
+  check_device_range(idx, sizeof(long long) * n, device_, "scatter_halo: index buffer");
+  check_device_range(v, sizeof(double) * n, device_, "scatter_halo: value buffer");
+  ck(cudaMemsetAsync(scalar_, 0, sizeof(unsigned long long), stream_), "memset");
+  launch_scatter_values(st_[live_].c[comp], idx, v, n, g_.size(), scalar_, stream_);
+  check_cuda("scatter launch");
+  unsigned long long bad = 0;
+  ck(cudaMemcpyAsync(&bad, scalar_, sizeof bad, cudaMemcpyDeviceToHost, stream_), "scatter flag");
+  ck(cudaStreamSynchronize(stream_), "scatter");
+  if (bad & 1ull)
+    throw std::invalid_argument("MhdSolver2D::scatter_halo: storage index out of range");
+  if (bad & 2ull) throw std::invalid_argument("MhdSolver2D::scatter_halo: non-finite value");
   if (!seeded_dirty_) halo_write_ = solver_owned_;
   seeded_dirty_ = true;
   front_order_ = 0;

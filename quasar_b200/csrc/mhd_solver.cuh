@@ -94,6 +94,14 @@ class MhdSolver2D {
   // stays solver-owned and its preflight stays the one of a stepped state.
   void set_owned_window(int x0, int x1, int y0, int y1);
   void write_halo(int comp, const double* host, long long n);
+  // The same exchange on the device: gather_live copies the live values at
+  // storage indices idx[0..n) into out; scatter_halo writes v[k] to index
+  // idx[k] (all finite; on any bad index or value it writes nothing and
+  // throws) and keeps the state solver-owned like write_halo.  idx, out and
+  // v are device memory of the solver's device, ready when called; both
+  // return after the copy finished.
+  void gather_live(int comp, const long long* idx, long long n, double* out);
+  void scatter_halo(int comp, const long long* idx, long long n, const double* v);
 
  private:
   friend class MhdBatch2D;  // batched stage launches over the same registers
@@ -118,6 +126,7 @@ class MhdSolver2D {
 
   Config cfg_;
   Grid g_;
+  int device_ = 0;
   cudaStream_t stream_ = nullptr;
   double* arena_ = nullptr;
   int* iarena_ = nullptr;

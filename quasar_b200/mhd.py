@@ -115,6 +115,18 @@ class MhdConfig:
     background: MhdBackgroundSpec = field(default_factory=MhdBackgroundSpec)
 
 
+def _check_device_pair(idx, vals, what: str) -> None:
+    import torch
+    if not (isinstance(idx, torch.Tensor) and isinstance(vals, torch.Tensor)):
+        raise TypeError(f"{what}: idx and values must be torch tensors")
+    if idx.dtype != torch.int64 or vals.dtype != torch.float64:
+        raise TypeError(f"{what}: idx must be int64 and values float64")
+    if not (idx.is_cuda and vals.is_cuda and idx.is_contiguous() and vals.is_contiguous()):
+        raise ValueError(f"{what}: idx and values must be contiguous CUDA tensors")
+    if idx.numel() != vals.numel():
+        raise ValueError(f"{what}: idx and values differ in length")
+
+
 def _native_config(cfg: MhdConfig) -> _native.QmhdConfig:
     if cfg.geometry != "cartesian":
         raise ValueError("MhdSolver2D: geometry must be 'cartesian' in this library")
@@ -232,6 +244,22 @@ class MhdSolver2D:
         a = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1))
         _native.check(_native.lib().qmhd_solver_write_halo(
             self._h, component.encode(), a.ctypes.data, a.size))
+
+    def gather_live(self, component: str, idx, out) -> None:
+        """out[k] = live value of `component` at storage index idx[k]; idx
+        (int64) and out (float64) are contiguous CUDA tensors of the
+        solver's device."""
+        _check_device_pair(idx, out, "gather_live")
+        _native.check(_native.lib().qmhd_solver_gather_live(
+            self._h, component.encode(), idx.data_ptr(), idx.numel(), out.data_ptr()))
+
+    def scatter_halo(self, component: str, idx, values) -> None:
+        """Live value of `component` at storage index idx[k] = values[k]
+        (finite, from the solver's own steps); the state stays
+        solver-owned.  CUDA tensors as for gather_live."""
+        _check_device_pair(idx, values, "scatter_halo")
+        _native.check(_native.lib().qmhd_solver_scatter_halo(
+            self._h, component.encode(), idx.data_ptr(), idx.numel(), values.data_ptr()))
 
     def divergence_b_relative(self) -> float:
         """Dimensionless solenoidality: max |div B| x dx / max |B_face| over

@@ -23,9 +23,14 @@ undecomposed run.  What crosses ranks per step:
   error instead of leaving them waiting in the next collective.
 
 Positivity retries are not coordinated: a step that needs one on any rank
-raises on every rank.  The exchange goes through host buffers and the
-process group (gloo on the host, or NCCL with device tensors); the kernels
-never wait on another rank.
+raises on every rank.  The kernels never wait on another rank: the exchange
+is a host step between launches.  exchange="host" reads whole components
+back, patches the halo on the host and writes them with write_halo;
+exchange="device" gathers only the positions peers need into one packed
+device buffer per peer (gather_live), sends those buffers over the process
+group (CUDA tensors under NCCL, staged through host memory under gloo) and
+scatters the received ones into the halo (scatter_halo), so per step only
+the halo's bytes move.
 """
 from __future__ import annotations
 
@@ -210,9 +215,13 @@ class TiledSolver:
     method in the same order."""
 
     def __init__(self, cfg: mhd.MhdConfig, px: int, py: int, halo: int = DEFAULT_HALO,
-                 group=None, device: str = "cpu"):
+                 group=None, device: str = "cpu", exchange: str = "host"):
         import torch.distributed as dist
+        if exchange not in ("host", "device"):
+            raise ValueError("exchange must be 'host' or 'device'")
         self.dist, self.group, self.device = dist, group, device
+        self.exchange_mode = exchange
+        self._xplan = None
         self.rank = dist.get_rank(group)
         world = dist.get_world_size(group)
         g = cfg.grid
@@ -226,6 +235,11 @@ class TiledSolver:
         self.tile = self.layout.tiles[self.rank]
         self.local.set_owned_window(*self.tile.window())
         self.plans = [self.layout.exchange_plan(r, self.ng) for r in range(world)]
+        if exchange == "device":
+            import torch
+            # where the solver's state lives: the gathered and scattered halo
+            # values stay there; only the packed halo crosses the group
+            self.xdev = torch.device("cuda", torch.cuda.current_device())
 
     # ---- agreement and reductions -------------------------------------------
     def _reduce(self, value: float, op: str) -> float:
@@ -277,8 +291,107 @@ class TiledSolver:
         return t
 
     # ---- halo exchange ------------------------------------------------------
+    def _pairwise(self, sends, recvs) -> None:
+        """Blocking send / recv with every peer, pairwise in rank order: the
+        lower rank of a pair sends first, so no two ranks wait on each other."""
+        for p in sorted(set(sends) | set(recvs)):
+            if self.rank < p:
+                if p in sends:
+                    self.dist.send(sends[p], dst=p, group=self.group)
+                if p in recvs:
+                    self.dist.recv(recvs[p], src=p, group=self.group)
+            else:
+                if p in recvs:
+                    self.dist.recv(recvs[p], src=p, group=self.group)
+                if p in sends:
+                    self.dist.send(sends[p], dst=p, group=self.group)
+
     def exchange(self) -> None:
         """Refresh every local position another rank owns from that rank."""
+        if getattr(self, "exchange_mode", "host") == "device":
+            self._exchange_device()
+        else:
+            self._exchange_host()
+
+    def _device_plan(self):
+        """The exchange plan as device index tensors, built once: per peer
+        the (component, indices) this rank packs for it and unpacks from it,
+        in the agreed order (components in COMPONENTS order, positions in the
+        receiver's order), and the periodic self-images."""
+        if self._xplan is not None:
+            return self._xplan
+        import torch
+        kinds = {n: self.layout.kind_of(n) for n in COMPONENTS}
+
+        def dev(a):
+            return torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=self.xdev)
+        send, recv, images = {}, {}, []
+        for p in range(self.layout.world):
+            if p == self.rank:
+                continue
+            need = self.plans[p].get(self.rank, {})
+            items = [(n, dev(need[kinds[n]][1])) for n in COMPONENTS if kinds[n] in need]
+            if items:
+                send[p] = items
+        mine = self.plans[self.rank]
+        for p, have in mine.items():
+            items = [(n, dev(have[kinds[n]][0])) for n in COMPONENTS if kinds[n] in have]
+            if p == self.rank:
+                images = [(n, dev(have[kinds[n]][1]), idx) for n, idx in items]
+            elif items:
+                recv[p] = items
+        self._xplan = (send, recv, images)
+        return self._xplan
+
+    def _sync(self) -> None:
+        import torch
+        if self.xdev.type == "cuda":
+            torch.cuda.synchronize(self.xdev)
+
+    def _exchange_device(self) -> None:
+        """The exchange without whole components crossing to the host: each
+        rank gathers what its peers need into one packed device buffer per
+        peer, the buffers cross the group (directly as CUDA tensors under
+        NCCL, staged through host memory under gloo), and the receiver
+        scatters them into its halo positions."""
+        import torch
+        send, recv, images = self._device_plan()
+        f64 = torch.float64
+        packed, image_vals = {}, []
+
+        def pack():
+            self._sync()
+            for p, items in send.items():
+                buf = torch.empty(sum(int(i.numel()) for _, i in items), dtype=f64,
+                                  device=self.xdev)
+                off = 0
+                for n, idx in items:
+                    self.local.gather_live(n, idx, buf[off:off + idx.numel()])
+                    off += idx.numel()
+                packed[p] = buf
+            for n, src, dst in images:
+                v = torch.empty(src.numel(), dtype=f64, device=self.xdev)
+                self.local.gather_live(n, src, v)
+                image_vals.append((n, dst, v))
+        self._agree(pack)
+        sends = {p: b.to(self.device) for p, b in packed.items()}
+        recvs = {p: torch.empty(sum(int(i.numel()) for _, i in items), dtype=f64,
+                                device=self.device) for p, items in recv.items()}
+        self._pairwise(sends, recvs)
+
+        def unpack():
+            bufs = {p: b.to(self.xdev) for p, b in recvs.items()}
+            self._sync()
+            for p, items in recv.items():
+                off = 0
+                for n, idx in items:
+                    self.local.scatter_halo(n, idx, bufs[p][off:off + idx.numel()])
+                    off += idx.numel()
+            for n, dst, v in image_vals:
+                self.local.scatter_halo(n, dst, v)
+        self._agree(unpack)
+
+    def _exchange_host(self) -> None:
         import torch
         arrays = {n: self.local.state_component_to_host(n) for n in COMPONENTS}
         world = self.layout.world
@@ -299,18 +412,7 @@ class TiledSolver:
                 continue
             size = sum(len(mine[p][kinds[n]][0]) for n in COMPONENTS if kinds[n] in mine[p])
             recvs[p] = torch.empty(size, dtype=torch.float64, device=self.device)
-        # pairwise in rank order: lower rank sends first, so gloo never deadlocks
-        for p in sorted(set(sends) | set(recvs)):
-            if self.rank < p:
-                if p in sends:
-                    self.dist.send(sends[p], dst=p, group=self.group)
-                if p in recvs:
-                    self.dist.recv(recvs[p], src=p, group=self.group)
-            else:
-                if p in recvs:
-                    self.dist.recv(recvs[p], src=p, group=self.group)
-                if p in sends:
-                    self.dist.send(sends[p], dst=p, group=self.group)
+        self._pairwise(sends, recvs)
         for p, buf in recvs.items():
             data, off = buf.cpu().numpy(), 0
             for n in COMPONENTS:

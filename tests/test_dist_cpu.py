@@ -134,8 +134,19 @@ class _ArraySolver:
     def write_halo(self, name, values):
         self.arrays[name] = np.asarray(values, dtype=np.float64).copy()
 
+    # the device exchange's calls, on CPU tensors
+    def gather_live(self, name, idx, out):
+        import torch
+        out.copy_(torch.from_numpy(self.arrays[name])[idx])
 
-def _tile_rank(rank, world, port, q, nx, ny, bc, px, py, halo):
+    def scatter_halo(self, name, idx, values):
+        v = values.numpy()
+        if not np.all(np.isfinite(v)):
+            raise ValueError("scatter_halo: non-finite value")
+        self.arrays[name][idx.numpy()] = v
+
+
+def _tile_rank(rank, world, port, q, nx, ny, bc, px, py, halo, mode):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
                       WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
     sys.path.insert(0, ROOT)
@@ -164,6 +175,10 @@ def _tile_rank(rank, world, port, q, nx, ny, bc, px, py, halo):
     ts.layout, ts.tile, ts.ng = lay, t, ng
     ts.local = _ArraySolver(loc)
     ts.plans = [lay.exchange_plan(r, ng) for r in range(world)]
+    ts.exchange_mode, ts._xplan = mode, None
+    if mode == "device":
+        import torch
+        ts.xdev = torch.device("cpu")
     ts.exchange()
     ok = True
     for n in tiles.COMPONENTS:
@@ -186,24 +201,28 @@ def _tile_rank(rank, world, port, q, nx, ny, bc, px, py, halo):
     q.put((rank, bool(ok), bool(gat)))
 
 
+@pytest.mark.parametrize("mode", ["host", "device"])
 @pytest.mark.parametrize("nx,ny,bc,px,py,halo", [
     (24, 20, ("periodic",) * 4, 2, 1, 6),
     (24, 20, ("outflow",) * 4, 1, 2, 5),
     (17, 13, ("periodic", "periodic", "outflow", "outflow"), 2, 2, 4),
     (10, 12, ("periodic",) * 4, 2, 2, 7),   # halos wider than a tile: periodic images
 ])
-def test_tile_halo_exchange_over_gloo(nx, ny, bc, px, py, halo):
+def test_tile_halo_exchange_over_gloo(nx, ny, bc, px, py, halo, mode):
     """The tile runtime's exchange (quasar_b200/tiles.py) on gloo ranks with
     numpy arrays in place of the solvers: every position a tile does not own
     (cells and both face fields, periodic images included) comes back equal
     to the whole domain's value, and gathering the owned values rebuilds the
-    whole domain."""
+    whole domain.  "device" runs the packed gather / send / scatter exchange
+    with CPU tensors standing in for the device buffers (the stale positions
+    hold NaN, so a position the plan missed or scattered twice from a stale
+    source shows)."""
     import torch.multiprocessing as mp
     world = px * py
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_tile_rank, args=(r, world, port, q, nx, ny, bc, px, py, halo))
+    procs = [ctx.Process(target=_tile_rank, args=(r, world, port, q, nx, ny, bc, px, py, halo, mode))
              for r in range(world)]
     for p in procs:
         p.start()

@@ -38,7 +38,7 @@ def _config(case, n, order, bc):
     return cfg
 
 
-def _rank(rank, world, port, q, case, n, order, bc, px, py, steps):
+def _rank(rank, world, port, q, case, n, order, bc, px, py, steps, exchange):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
                       WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
     sys.path.insert(0, ROOT)
@@ -52,7 +52,7 @@ def _rank(rank, world, port, q, case, n, order, bc, px, py, steps):
                             timeout=datetime.timedelta(seconds=120))
     cfg = _config(case, n, order, bc)
     glob = ics.GENERATORS[case](n, order=order)
-    ts = tiles.TiledSolver(cfg, px, py)
+    ts = tiles.TiledSolver(cfg, px, py, exchange=exchange)
     for name, a in zip(ics.COMPONENTS, glob):
         ts.seed_global(name, a)
     dts = []
@@ -91,20 +91,23 @@ def _rank(rank, world, port, q, case, n, order, bc, px, py, steps):
     q.put((rank, result))
 
 
-@pytest.mark.parametrize("case,n,order,bc,px,py,exact", [
-    ("rotor", 160, 7, "outflow", 2, 2, True),
-    ("blast", 144, 7, "outflow", 1, 2, True),
-    ("orszag_tang", 128, 5, "periodic", 2, 1, False),
-    ("orszag_tang", 96, 7, "periodic", 2, 2, False),
+@pytest.mark.parametrize("case,n,order,bc,px,py,exact,exchange", [
+    ("rotor", 160, 7, "outflow", 2, 2, True, "host"),
+    ("blast", 144, 7, "outflow", 1, 2, True, "host"),
+    ("orszag_tang", 128, 5, "periodic", 2, 1, False, "host"),
+    ("orszag_tang", 96, 7, "periodic", 2, 2, False, "host"),
+    ("rotor", 160, 7, "outflow", 2, 2, True, "device"),
+    ("orszag_tang", 96, 7, "periodic", 2, 2, False, "device"),
 ])
-def test_tiles_match_the_undecomposed_step(case, n, order, bc, px, py, exact):
+def test_tiles_match_the_undecomposed_step(case, n, order, bc, px, py, exact, exchange):
     import torch.multiprocessing as mp
     world = px * py
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
     steps = 5
-    procs = [ctx.Process(target=_rank, args=(r, world, port, q, case, n, order, bc, px, py, steps))
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q, case, n, order, bc, px, py, steps,
+                                                exchange))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -119,3 +122,55 @@ def test_tiles_match_the_undecomposed_step(case, n, order, bc, px, py, exact):
     else:
         assert all(abs(a - b) <= 1e-12 * b for a, b in zip(dts, ref_dts)), (dts, ref_dts)
         assert rel <= 1e-12, (rel, same)
+
+
+def test_device_exchange_calls_check_their_buffers():
+    """gather_live / scatter_halo: values land at the given storage
+    indices; a bad index or a non-finite value fails the scatter with
+    nothing written; host memory and buffers past their allocation are
+    refused before any launch."""
+    sys.path.insert(0, ROOT)
+    import torch
+
+    from quasar_b200 import _native, ics, mhd
+    n, order = 64, 5
+    cfg = _config("rotor", n, order, "outflow")
+    s = mhd.MhdSolver2D(cfg)
+    glob = ics.GENERATORS["rotor"](n, order=order)
+    for name, a in zip(ics.COMPONENTS, glob):
+        s.seed_state(name, a)
+    s.step_unchecked(s.cfl_limit())
+    dev = torch.device("cuda", torch.cuda.current_device())
+    size = s.grid().storage_size()
+    rho = s.state_component_to_host("rho")
+    idx = torch.tensor([0, 5, size // 2, size - 1], dtype=torch.int64, device=dev)
+    out = torch.empty(4, dtype=torch.float64, device=dev)
+    s.gather_live("rho", idx, out)
+    assert np.array_equal(out.cpu().numpy(), rho[idx.cpu().numpy()])
+    vals = torch.tensor([1.5, 2.5, 3.5, 4.5], dtype=torch.float64, device=dev)
+    s.scatter_halo("rho", idx, vals)
+    got = s.state_component_to_host("rho")
+    assert np.array_equal(got[idx.cpu().numpy()], vals.cpu().numpy())
+    before = got.copy()
+    bad_idx = torch.tensor([1, size], dtype=torch.int64, device=dev)
+    with pytest.raises(ValueError, match="out of range"):
+        s.scatter_halo("rho", bad_idx, vals[:2])
+    bad_val = torch.tensor([1.0, float("nan")], dtype=torch.float64, device=dev)
+    with pytest.raises(ValueError, match="non-finite"):
+        s.scatter_halo("rho", idx[:2], bad_val)
+    assert np.array_equal(s.state_component_to_host("rho"), before)
+    with pytest.raises(ValueError, match="out of range"):
+        s.gather_live("rho", bad_idx, out[:2])
+    # past the end of the allocation (the whole caching-allocator segment)
+    big = torch.empty(1 << 20, dtype=torch.float64, device=dev)
+    tail = big[-2:]
+    with pytest.raises(ValueError):
+        _native.check(_native.lib().qmhd_solver_gather_live(
+            s._h, b"rho", idx.data_ptr(), 1 << 22, tail.data_ptr()))
+    host_idx = np.zeros(4, dtype=np.int64)
+    with pytest.raises(ValueError, match="not device memory"):
+        _native.check(_native.lib().qmhd_solver_gather_live(
+            s._h, b"rho", host_idx.ctypes.data, 4, out.data_ptr()))
+    # the state is still a stepped one: the next step runs
+    s.scatter_halo("rho", idx, torch.from_numpy(before[idx.cpu().numpy()]).to(dev))
+    s.step_unchecked(s.cfl_limit())
