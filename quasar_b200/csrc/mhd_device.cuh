@@ -230,14 +230,19 @@ __device__ __forceinline__ bool recon_admissible(const St& s, double gamma) {
   return isfinite(s.mx) && isfinite(s.my) && isfinite(s.mz) && isfinite(s.E) &&
          isfinite(s.bx) && isfinite(s.by) && isfinite(s.bz);
 }
-// mhd_face_quadrature.hpp:68-76
-__device__ __forceinline__ bool point_admissible(const St& s, double gamma) {
-  if (!(isfinite(s.rho) && s.rho > 0.0 && isfinite(s.mx) && isfinite(s.my) &&
-        isfinite(s.mz) && isfinite(s.E) && isfinite(s.bx) && isfinite(s.by) &&
-        isfinite(s.bz)))
-    return false;
-  const double p = pressure_f(s, gamma, 1.0 / s.rho);
+// mhd_face_quadrature.hpp:68-76, with 1/rho supplied.  Every component
+// enters the pressure, so with rho finite and positive "p finite and
+// positive" already fails for any non-finite component (an infinite momentum
+// or field drives p to -inf, an infinite energy to +/-inf, a NaN to NaN): the
+// reference's per-component finiteness tests are implied and not repeated,
+// the decision is the same.
+__device__ __forceinline__ bool point_admissible_ir(const St& s, double gamma, double ir) {
+  if (!(isfinite(s.rho) && s.rho > 0.0)) return false;
+  const double p = pressure_f(s, gamma, ir);
   return isfinite(p) && p > 0.0;
+}
+__device__ __forceinline__ bool point_admissible(const St& s, double gamma) {
+  return point_admissible_ir(s, gamma, 1.0 / s.rho);
 }
 
 // ---- MP limiter: numerics/mp_limiter.hpp ---------------------------------
@@ -384,10 +389,12 @@ __device__ __forceinline__ bool same_state(const St& a, const St& b) {
          a.bx == b.bx && a.by == b.by && a.bz == b.bz;
 }
 
-// hlld_core.hpp:213-457 (B0 inactive).
-__device__ __forceinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double gamma) {
+// hlld_core.hpp:213-457 (B0 inactive), with the reciprocal densities of the
+// two states supplied (irl = 1 / Lin.rho, irr = 1 / Rin.rho).
+__device__ __forceinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double gamma,
+                                          double irl, double irr) {
   const double rel = 64.0 * kEps;
-  if (same_state(Lin, Rin)) return physical_flux_x(Lin, gamma);
+  if (same_state(Lin, Rin)) return physical_flux_xp(Lin, pressure_f(Lin, gamma, irl), irl);
   const double bn = 0.5 * Lin.bx + 0.5 * Rin.bx;
   St L = Lin, R = Rin;
   const double hbn2 = 0.5 * (bn * bn);
@@ -397,7 +404,6 @@ __device__ __forceinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double g
   R.bx = bn;
   const bool bn2_ok = hbn2 <= 0.5 * 1.7976931348623157e308;
   const double bn2 = bn2_ok ? 2.0 * hbn2 : 0.0;
-  const double irl = 1.0 / L.rho, irr = 1.0 / R.rho;
   const double vxL = L.mx * irl, vyL = L.my * irl, vzL = L.mz * irl;
   const double vxR = R.mx * irr, vyR = R.my * irr, vzR = R.mz * irr;
   const double pL = pressure_f(L, gamma, irl), pR = pressure_f(R, gamma, irr);
@@ -536,12 +542,18 @@ __device__ __forceinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double g
   return f;
 }
 
-// Face-normal Riemann flux in the lab frame (mhd_face_quadrature.hpp:173-185).
+__device__ __forceinline__ Fx hlld_flux_x(const St& Lin, const St& Rin, double gamma) {
+  return hlld_flux_x(Lin, Rin, gamma, 1.0 / Lin.rho, 1.0 / Rin.rho);
+}
+
+// Face-normal Riemann flux in the lab frame (mhd_face_quadrature.hpp:173-185),
+// irl / irr = 1 / rho of the two states.
 template <int DIR>
-__device__ __forceinline__ Fx riemann(const St& l, const St& r, bool lf, double gamma) {
+__device__ __forceinline__ Fx riemann(const St& l, const St& r, bool lf, double gamma,
+                                      double irl, double irr) {
   const St a = DIR == 0 ? l : swap_xy(l);
   const St b = DIR == 0 ? r : swap_xy(r);
-  Fx f = lf ? lf_flux_x(a, b, gamma) : hlld_flux_x(a, b, gamma);
+  Fx f = lf ? lf_flux_x(a, b, gamma) : hlld_flux_x(a, b, gamma, irl, irr);
   if (DIR == 1) {
     const double t = f.mx;
     f.mx = f.my;
@@ -551,6 +563,10 @@ __device__ __forceinline__ Fx riemann(const St& l, const St& r, bool lf, double 
     f.by = u;
   }
   return f;
+}
+template <int DIR>
+__device__ __forceinline__ Fx riemann(const St& l, const St& r, bool lf, double gamma) {
+  return riemann<DIR>(l, r, lf, gamma, 1.0 / l.rho, 1.0 / r.rho);
 }
 
 // ---- transverse quadrature: numerics/finite_volume_quadrature.hpp:12-68 --

@@ -399,9 +399,18 @@ struct Eg {
 };
 constexpr double kRs2 = 0.7071067811865475;  // 1/sqrt(2) rounded
 
+// The magnetosonic speeds and the fast / slow normalisations keep the
+// reference's scaled forms and uncontracted products: where the transverse
+// field vanishes, af^2 is a difference of nearly equal squares and af its
+// square root, so a one-ulp change of any input moves af by ~1e-8 and the
+// face states by ~1e-11.  Quantities that feed only the eigenvector
+// entries (velocities, transverse unit vector, 1/a^2, |v|^2/2) share one
+// reciprocal each instead of a division per term (a rounding-level
+// difference).
 __device__ __forceinline__ Eg eig_scalars(const St& s, double gamma) {
   Eg e;
-  const Pr w = to_prim(s, gamma);
+  const double ir = 1.0 / s.rho;
+  const Pr w{s.rho, s.mx * ir, s.my * ir, s.mz * ir, pressure(s, gamma), s.bx, s.by, s.bz};
   e.rho = w.rho;
   const double p = w.p > 0.0 ? w.p : 0.0;
   e.sr = sqrt(e.rho);
@@ -430,19 +439,21 @@ __device__ __forceinline__ Eg eig_scalars(const St& s, double gamma) {
       e.b1 = kRs2;
       e.b2 = kRs2;
     } else {
-      e.b1 = w.by / bt;
-      e.b2 = w.bz / bt;
+      const double ibt = 1.0 / bt;
+      e.b1 = w.by * ibt;
+      e.b2 = w.bz * ibt;
     }
   }
   e.sbn = w.bx >= 0.0 ? 1.0 : -1.0;
   e.vn = w.vx;
   e.vt1 = w.vy;
   e.vt2 = w.vz;
-  e.ia2 = e.a > 0.0 ? (1.0 / e.a) / e.a : 0.0;
+  const double ia = e.a > 0.0 ? 1.0 / e.a : 0.0;
+  e.ia2 = ia * ia;
   e.ra2 = gamma * p;
   e.gm1 = gamma - 1.0;
-  e.hv2 = half_sq3(e.vn, e.vt1, e.vt2);
-  e.ir = 1.0 / e.rho;
+  e.hv2 = 0.5 * ((e.vn * e.vn + e.vt1 * e.vt1) + e.vt2 * e.vt2);
+  e.ir = ir;
   e.isr = 1.0 / e.sr;
   e.igm = 1.0 / e.gm1;
   return e;
@@ -731,12 +742,17 @@ __device__ __forceinline__ void finish_face(const Grid& g, const StateP& u, cons
 // one wavefront per half-warp whether or not the lanes share its address.
 //
 // Per-warp shared memory (doubles): a face record [kRec][32] and eight group
-// buffers R[7][7] followed by delta[8][7], whose first 14 slots later hold
-// the projected face values w[2][7].
+// buffers R[7][8] followed by delta[8][7], whose first 14 slots later hold
+// the projected face values w[2][7].  The R columns are padded to eight
+// doubles so that the L R = I check reads them as 16-byte pairs (half the
+// load instructions of scalar reads: the check went 41.6 -> 39.7 ms per
+// rotor 4096^2 MP7 step of reconstruction); the group stride of 114 doubles
+// puts the eight groups' 16-byte reads on distinct banks.  Padding the
+// stencil deltas the same way measured no faster.
 constexpr int kRecC = 0;    // canonical reference state, 8 components
 constexpr int kRecE = 8;    // 17 eigen scalars, later dl[7] and dr[7]
 constexpr int kRec = 25;
-constexpr int kGrpR = 0, kGrpD = 49, kGrpW = 49, kGrpDoubles = 105;
+constexpr int kGrpR = 0, kRS = 8, kGrpD = 56, kGrpW = 56, kGrpDoubles = 114;
 constexpr int kGroups = 8;
 constexpr int kWarpReconDoubles = kRec * 32 + kGroups * kGrpDoubles;
 constexpr int kReconWarps = 4;
@@ -884,10 +900,10 @@ __device__ void mp_faces_warp(const Grid& g, const StateP& u, const IfaceP& out,
       wave_lr(e, ka, La, Ra);
       wave_lr(e, kb, Lb, Rb);
 #pragma unroll
-      for (int m = 0; m < 7; ++m) grp[kGrpR + ka * 7 + m] = Ra[m];
+      for (int m = 0; m < 7; ++m) grp[kGrpR + ka * kRS + m] = Ra[m];
       if (two) {
 #pragma unroll
-        for (int m = 0; m < 7; ++m) grp[kGrpR + kb * 7 + m] = Rb[m];
+        for (int m = 0; m < 7; ++m) grp[kGrpR + kb * kRS + m] = Rb[m];
       }
     }
     __syncwarp();
@@ -897,9 +913,9 @@ __device__ void mp_faces_warp(const Grid& g, const StateP& u, const IfaceP& out,
     if (on) {
 #pragma unroll
       for (int jc = 0; jc < 7; ++jc) {
-        double R7[7];
-#pragma unroll
-        for (int m = 0; m < 7; ++m) R7[m] = grp[kGrpR + jc * 7 + m];
+        const double2* R2 = reinterpret_cast<const double2*>(grp + kGrpR + jc * kRS);
+        const double2 p0 = R2[0], p1 = R2[1], p2 = R2[2], p3 = R2[3];
+        const double R7[7] = {p0.x, p0.y, p1.x, p1.y, p2.x, p2.y, p3.x};
         double da = 0.0, db = 0.0;
 #pragma unroll
         for (int m = 0; m < 7; ++m) {
@@ -917,8 +933,8 @@ __device__ void mp_faces_warp(const Grid& g, const StateP& u, const IfaceP& out,
       for (int v = 0; v < 7; ++v) {
         La[v] = v == ka ? 1.0 : 0.0;
         Lb[v] = v == kb ? 1.0 : 0.0;
-        grp[kGrpR + ka * 7 + v] = v == ka ? 1.0 : 0.0;
-        if (two) grp[kGrpR + kb * 7 + v] = v == kb ? 1.0 : 0.0;
+        grp[kGrpR + ka * kRS + v] = v == ka ? 1.0 : 0.0;
+        if (two) grp[kGrpR + kb * kRS + v] = v == kb ? 1.0 : 0.0;
       }
     }
     // stencil deltas in the canonical frame: lane rl loads cells rl, rl + 4
@@ -989,7 +1005,7 @@ __device__ void mp_faces_warp(const Grid& g, const StateP& u, const IfaceP& out,
           double dl = 0.0, dr = 0.0;
 #pragma unroll
           for (int q = 0; q < 7; ++q) {
-            const double rq = grp[kGrpR + q * 7 + v];
+            const double rq = grp[kGrpR + q * kRS + v];
             dl += rq * grp[kGrpW + q];
             dr += rq * grp[kGrpW + 7 + q];
           }
@@ -1489,8 +1505,11 @@ constexpr int kFqTX = 8, kFqTY = 4;
 constexpr int kFqThreads = 4 * kFqTX * kFqTY;
 template <int ORDER>
 constexpr int fq_ty() { return ORDER == 5 ? 5 : 4; }
-// 96 registers, no spills: five 128-thread blocks per SM measured 8-11%
-// faster than four at 128 registers (six spill and lose it again)
+// 96 registers (ptxas keeps a few values of the HLLD tail on the stack):
+// five 128-thread blocks per SM measured 8-11% faster than four at 128
+// registers (six spill more and lose it again).  Staging the tile
+// face-major so that lanes read component pairs as 16-byte loads measured
+// 9% slower (more spills at this register cap).
 constexpr int kFqBlocksPerSm = 5;
 
 // TX: faces per tile row; the block is four warps of 32 / Q groups each.
@@ -1551,6 +1570,7 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
   auto tr = [&](int t) { return DIR == 0 ? fy + t : fy; };
   auto tcl = [&](int t) { return DIR == 0 ? fx : fx + t; };
   St l{}, r{};
+  double irl = 1.0, irr = 1.0;
   bool ok = true;
   {
     double w[N];
@@ -1570,7 +1590,9 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
     }
     l = St{pl[0], pl[1], pl[2], pl[3], pl[4], pl[5], pl[6], pl[7]};
     r = St{pr[0], pr[1], pr[2], pr[3], pr[4], pr[5], pr[6], pr[7]};
-    ok = point_admissible(l, gamma) && point_admissible(r, gamma);
+    irl = 1.0 / l.rho;
+    irr = 1.0 / r.rho;
+    ok = point_admissible_ir(l, gamma, irl) && point_admissible_ir(r, gamma, irr);
   }
   auto centre = [&](bool left) {
     const int o = left ? 0 : 8, rr = tr(H), cc = tcl(H);
@@ -1589,10 +1611,12 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
   if (!group_ok) {
     l = centre(true);
     r = centre(false);
+    irl = 1.0 / l.rho;
+    irr = 1.0 / r.rho;
   }
   double fv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (solve) {
-    const Fx f = riemann<DIR>(l, r, kLF, gamma);
+    const Fx f = riemann<DIR>(l, r, kLF, gamma, irl, irr);
     fv[0] = f.rho; fv[1] = f.mx; fv[2] = f.my; fv[3] = f.mz;
     fv[4] = f.E;   fv[5] = f.bx; fv[6] = f.by; fv[7] = f.bz;
   }
@@ -1666,10 +1690,14 @@ __global__ void __launch_bounds__(kFqThreads, kFqBlocksPerSm)
 namespace {
 
 // E_z = -(v x B)_z (mhd_ct.hip:408-417, zero background)
-__device__ __forceinline__ double physical_ez(const St& s) {
-  const double vx = s.mx / s.rho, vy = s.my / s.rho;
+// E_z = -(v x B)_z from the state and its 1/rho (one reciprocal shared with
+// the point's admissibility test instead of a division per velocity
+// component: a rounding-level difference)
+__device__ __forceinline__ double physical_ez_ir(const St& s, double ir) {
+  const double vx = s.mx * ir, vy = s.my * ir;
   return __dadd_rn(__dmul_rn(vy, s.bx), __dmul_rn(vx, -s.by));
 }
+__device__ __forceinline__ double physical_ez(const St& s) { return physical_ez_ir(s, 1.0 / s.rho); }
 
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
@@ -1721,8 +1749,9 @@ __global__ void __launch_bounds__(128) k_cell_emf(Grid g, StateP u, double* cell
                      point_value<ORDER>(qy, rows[2]), point_value<ORDER>(qy, rows[3]),
                      point_value<ORDER>(qy, rows[4]), point_value<ORDER>(qy, rows[5]),
                      point_value<ORDER>(qy, rows[6]), point_value<ORDER>(qy, rows[7])};
-          if (!point_admissible(p, gamma)) ok = false;
-          pt[qy][qx] = physical_ez(p);
+          const double ir = 1.0 / p.rho;
+          if (!point_admissible_ir(p, gamma, ir)) ok = false;
+          pt[qy][qx] = physical_ez_ir(p, ir);
         }
       }
       if (ok) {
@@ -1873,16 +1902,28 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
 #pragma unroll
     for (int t = 0; t < N; ++t) wx[t] = point_w<ORDER>(qx, t);
     // x-recovery of every staged row (component c, row r) at this x node:
-    // row task t = c * SY + r, TY of them at a time, lane = column
-    static_assert((8 * SY) % TY == 0, "row tasks divide evenly over the block's rows");
+    // task = (row t = c * SY + r, column pair p); the two outputs' N + 1
+    // taps come in as 16-byte loads (the staged rows start on 16 bytes;
+    // with XO = 1 the pair's taps start one double into the first load)
+    static_assert(RS % 2 == 0 && TX % 2 == 0, "16-byte rows");
+    constexpr int NL = (XO + N + 2) / 2;  // 16-byte loads per pair
+    for (int tk = tid; tk < 8 * SY * (TX / 2); tk += TX * TY) {
+      const int t = tk / (TX / 2), pr = tk - t * (TX / 2);
+      const double2* row = reinterpret_cast<const double2*>(S + t * RS + 2 * pr);
+      double v[2 * NL];
 #pragma unroll
-    for (int m = 0; m < 8 * SY / TY; ++m) {
-      const int t = threadIdx.y + m * TY;
-      const double* row = S + t * RS + XO + threadIdx.x;
-      double smp[N];
+      for (int q = 0; q < NL; ++q) {
+        const double2 d = row[q];
+        v[2 * q] = d.x;
+        v[2 * q + 1] = d.y;
+      }
+      double s0[N], s1[N];
 #pragma unroll
-      for (int q = 0; q < N; ++q) smp[q] = row[q];
-      X[t * TX + threadIdx.x] = wsum<N>(wx, smp);
+      for (int q = 0; q < N; ++q) {
+        s0[q] = v[XO + q];
+        s1[q] = v[XO + 1 + q];
+      }
+      reinterpret_cast<double2*>(X + t * TX)[pr] = make_double2(wsum<N>(wx, s0), wsum<N>(wx, s1));
     }
     __syncthreads();
     if (active && ok) {
@@ -1899,8 +1940,9 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
       for (int qy = 0; qy < Q; ++qy) {
         const St p{st[qy][0], st[qy][1], st[qy][2], st[qy][3],
                    st[qy][4], st[qy][5], st[qy][6], st[qy][7]};
-        if (!point_admissible(p, gamma)) ok = false;
-        pt[qy][qx] = physical_ez(p);
+        const double ir = 1.0 / p.rho;
+        if (!point_admissible_ir(p, gamma, ir)) ok = false;
+        pt[qy][qx] = physical_ez_ir(p, ir);
       }
     }
     __syncthreads();
@@ -2058,6 +2100,13 @@ __device__ __forceinline__ void b_corner_emf_s(const Grid& g, const double* cell
   __shared__ double tile[TH][TW];
   __shared__ double sxe[TH][32], sye[4][TW];
   __shared__ int sxn[TH][32], syn[4][TW];
+  // separable centred value: each tile row's x-interpolation at the block's
+  // 32 corner columns (xr), whether that row is constant over the corner's
+  // x-stencil (xc), and whether each tile column is constant over the y-
+  // stencil of each of the 4 corner rows (yc); every corner then reads NT of
+  // each instead of its NT x NT cells (same sums, same order)
+  __shared__ double xr[TH][32];
+  __shared__ unsigned char xc[TH][32], yc[4][TW];
   if (ctl->status) return;  // uniform over the block
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
   const int i0 = bx * 32, j0 = by * 4;
@@ -2082,6 +2131,26 @@ __device__ __forceinline__ void b_corner_emf_s(const Grid& g, const double* cell
     const long long ky = g.idx(mi, fj);
     sye[b][a] = __ldg(yemf + ky);
     syn[b][a] = __ldg(ynj + ky);
+  }
+  __syncthreads();
+  for (int t = tid; t < TH * 32; t += 128) {
+    const int a = t % 32, b = t / 32;
+    double c[NT];
+#pragma unroll
+    for (int p = 0; p < NT; ++p) c[p] = tile[b][a + p];
+    bool cst = true;
+#pragma unroll
+    for (int p = 1; p < NT; ++p) cst = cst && (c[p] == c[0]);
+    xr[b][a] = edge_interp<NT>(c);
+    xc[b][a] = cst;
+  }
+  for (int t = tid; t < 4 * TW; t += 128) {
+    const int a = t % TW, b = t / TW;
+    const double c0 = tile[b][a];
+    bool cst = true;
+#pragma unroll
+    for (int q = 1; q < NT; ++q) cst = cst && (tile[b + q][a] == c0);
+    yc[b][a] = cst;
   }
   __syncthreads();
   const int i = i0 + tx, j = j0 + ty;
@@ -2110,16 +2179,9 @@ __device__ __forceinline__ void b_corner_emf_s(const Grid& g, const double* cell
   bool const_x = true, const_y = true;
 #pragma unroll
   for (int q = 0; q < NT; ++q) {
-    double c[NT];
-#pragma unroll
-    for (int p = 0; p < NT; ++p) c[p] = tile[ty + q][tx + p];
-#pragma unroll
-    for (int p = 1; p < NT; ++p) const_x = const_x && (c[p] == c[0]);
-    if (q > 0) {
-#pragma unroll
-      for (int p = 0; p < NT; ++p) const_y = const_y && (c[p] == tile[ty][tx + p]);
-    }
-    line[q] = edge_interp<NT>(c);
+    line[q] = xr[ty + q][tx];
+    const_x = const_x && xc[ty + q][tx];
+    const_y = const_y && yc[ty][tx + q];
   }
   const double centred = edge_interp<NT>(line);
   const bool x_only = nj_y && const_y;
