@@ -2894,12 +2894,27 @@ __global__ void k_scatter_values(double* __restrict__ dst, const long long* __re
     dst[idx[k]] = v[k];
 }
 
+// Any non-finite value among v[0..n) sets *bad (which must start at zero).
+__global__ void k_flag_nonfinite(const double* __restrict__ v, long long n,
+                                 unsigned long long* bad) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  bool b = false;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += stride)
+    b = b || !isfinite(v[k]);
+  if (__any_sync(0xffffffffu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 1ull);
+}
+
 namespace {
 int exchange_blocks(long long n) {
   const long long b = (n + 255) / 256;
   return (int)(b < 4 * 148 ? (b > 0 ? b : 1) : 4 * 148);
 }
 }  // namespace
+
+void launch_flag_nonfinite(const double* v, long long n, unsigned long long* bad, cudaStream_t s) {
+  if (n <= 0) return;
+  k_flag_nonfinite<<<exchange_blocks(n), 256, 0, s>>>(v, n, bad);
+}
 
 void launch_gather_values(const double* src, const long long* idx, long long n, long long size,
                           double* out, unsigned long long* bad, cudaStream_t s) {

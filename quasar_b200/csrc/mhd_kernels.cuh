@@ -310,6 +310,9 @@ void launch_reconstruct_learned(const StageArgs& a, int dir, const unsigned char
 void launch_face_lists(const Grid& g, const unsigned char* flag, int* xlist, int* ylist,
                        int* counts, cudaStream_t s);
 
+// *bad |= 1 if any of v[0..n) is not finite (*bad must start at zero).
+void launch_flag_nonfinite(const double* v, long long n, unsigned long long* bad, cudaStream_t s);
+
 // ---- tile halo exchange ----------------------------------------------------
 // out[k] = src[idx[k]] and dst[idx[k]] = v[k] for k < n, indices checked
 // against [0, size) and scattered values against non-finite ones; problems

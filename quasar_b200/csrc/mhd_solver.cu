@@ -198,11 +198,23 @@ void MhdSolver2D::seed_state(int comp, const double* host, long long n) {
       << ") does not match the component storage size (" << g_.size() << ")";
     throw std::invalid_argument(m.str());
   }
-  for (long long k = 0; k < n; ++k)
-    if (!std::isfinite(host[k]))
-      throw std::invalid_argument(
-          "MhdSolver2D::seed_state: host buffer must contain only finite values");
-  ck(cudaMemcpyAsync(st_[live_].c[comp], host, sizeof(double) * n, cudaMemcpyHostToDevice,
+  // The values land in the first stage register (scratch between steps),
+  // are tested there on the device, and only then replace the live
+  // component, so a rejected buffer leaves the state as it was (a host-side
+  // scan of the buffer cost as much as the copy itself at large sizes).
+  double* stage = st_[s1_].c[comp];
+  ck(cudaMemcpyAsync(stage, host, sizeof(double) * n, cudaMemcpyHostToDevice, stream_),
+     "seed copy");
+  ck(cudaMemsetAsync(scalar_, 0, sizeof(unsigned long long), stream_), "memset");
+  launch_flag_nonfinite(stage, n, scalar_, stream_);
+  check_cuda("seed check launch");
+  unsigned long long bad = 0;
+  ck(cudaMemcpyAsync(&bad, scalar_, sizeof bad, cudaMemcpyDeviceToHost, stream_), "seed flag");
+  ck(cudaStreamSynchronize(stream_), "seed");
+  if (bad)
+    throw std::invalid_argument(
+        "MhdSolver2D::seed_state: host buffer must contain only finite values");
+  ck(cudaMemcpyAsync(st_[live_].c[comp], stage, sizeof(double) * n, cudaMemcpyDeviceToDevice,
                      stream_),
      "seed copy");
   ck(cudaStreamSynchronize(stream_), "seed");

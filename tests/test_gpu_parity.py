@@ -158,6 +158,15 @@ def test_error_behaviour_matches_reference():
     bad[0][5, 5] = np.nan
     with pytest.raises(ValueError):
         g.seed_state("rho", bad[0])
+    # a rejected buffer leaves the live state as it was (the values are
+    # tested on the device before they replace it), also after a step
+    seed(g, ic)
+    g.step_unchecked(g.cfl_limit())
+    before = g.state_component_to_host("rho")
+    bad[0][0, 0] = np.inf
+    with pytest.raises(ValueError, match="finite"):
+        g.seed_state("rho", bad[0])
+    assert np.array_equal(g.state_component_to_host("rho"), before)
     with pytest.raises(ValueError):
         g.seed_state("rho", ic[0][:-1])
     with pytest.raises(ValueError):
