@@ -19,6 +19,7 @@
 #include "quasar/numerics/hlld_core.hpp"
 #include "quasar/numerics/mhd_eigensystem.hpp"
 #include "quasar/numerics/mp_limiter.hpp"
+#include "quasar/numerics/mhd_background_metrics.hpp"
 #include "quasar/physics/mhd/kernels.hpp"
 
 #include <cstring>
@@ -137,6 +138,26 @@ int qref_step(void* h, double dt) {
 int qref_substeps(void* h) {
   return static_cast<MhdSolver2D*>(h)->last_positivity_substeps();
 }
+
+// The solver's own live-state solenoidality measure (the quantity
+// ensure_live_state_solenoidal, mhd_solver.cpp:1196-1222, compares with
+// numerics::kDiscreteSolenoidalTolerance) on the live register after the
+// boundary fill the preflight runs behind (mhd_solver.cpp:697-700), with the
+// provenance given explicitly: solver_owned = 1 is the test of a state the
+// solver stepped itself, 0 the stricter one of a seeded state.
+int qref_divb_relative(void* h, int solver_owned, double* out) {
+  try {
+    auto* s = static_cast<MhdSolver2D*>(h);
+    s->fill_ghosts(s->rk_[0]);
+    Real v = Real{0};
+    quasar::mhd::launch_mhd_ct_divb_relative_linf(s->rk_[0], s->divb_scratch_, &v, nullptr,
+                                                  s->is_cylindrical(), solver_owned != 0);
+    *out = v;
+    return 0;
+  } catch (const std::exception& e) { return fail(e); }
+}
+
+double qref_solenoidal_tolerance() { return quasar::numerics::kDiscreteSolenoidalTolerance; }
 
 int qref_divb(void* h, double* out) {
   try {

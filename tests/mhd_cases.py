@@ -186,6 +186,20 @@ class RefLib(_Lib):
                                   ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         L.qref_residual.argtypes = [ctypes.c_void_p] * 11
         L.qref_divb.argtypes = [ctypes.c_void_p, _dp]
+        if hasattr(L, "qref_divb_relative"):
+            L.qref_divb_relative.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+            L.qref_solenoidal_tolerance.restype = ctypes.c_double
+
+    def divb_relative(self, solver, solver_owned):
+        """The reference's live-state solenoidality measure of the solver's
+        live register, as a stepped (solver_owned) or a seeded state."""
+        v = ctypes.c_double()
+        if self.lib.qref_divb_relative(solver.h, int(solver_owned), ctypes.byref(v)) != 0:
+            raise RuntimeError(self.err())
+        return v.value
+
+    def solenoidal_tolerance(self):
+        return self.lib.qref_solenoidal_tolerance()
 
     def solver(self, nx, ny, order, gamma=5.0 / 3.0, cfl=0.4, bc=PERIODIC, lx=1.0, ly=1.0,
                ox=0.0, oy=0.0):

@@ -314,3 +314,52 @@ def test_background_queries_on_a_live_solver():
     assert g.has_background() is False
     with pytest.raises(RuntimeError, match="field-split background is not enabled"):
         g.seed_background("b0x", np.zeros(g.grid().storage_size()))
+
+
+def test_preflight_trip_is_the_reference_check():
+    """Orszag-Tang 2048^2 MP5: the plain step's live-state solenoidality
+    preflight stops the run after about a thousand steps (the smallest grid
+    where it trips; 1024^2 reaches t = 0.5).  Running the reference's CPU
+    build that far takes most of a day, so the state is handed to it
+    instead: the reference's own measure (oracle/_ref, the quantity
+    ensure_live_state_solenoidal compares, as a state the solver stepped)
+    rejects the state this solver rejected and accepts the last one it
+    stepped, against the reference's own tolerance."""
+    ref = M.RefLib()
+    if not hasattr(ref.lib, "qref_divb_relative"):
+        pytest.skip("reference build without the preflight entry point")
+    n, order = 2048, 5
+    ic = M.orszag_tang(n, order=order)
+    g = gpu_solver(n, order, M.PERIODIC)
+    seed(g, ic)
+    dts = []
+    for _ in range(3000):
+        try:
+            dt = g.cfl_limit()
+        except ValueError as e:
+            assert "divergence-free" in str(e), e
+            break
+        g.step_unchecked(dt)
+        dts.append(dt)
+    else:
+        pytest.fail("no preflight trip within 3000 steps")
+    rejected = [g.state_component_to_host(c) for c in M.COMPONENTS]
+    del g
+    # the last accepted state: the same steps again, one fewer
+    g2 = gpu_solver(n, order, M.PERIODIC)
+    seed(g2, ic)
+    for dt in dts[:-1]:
+        assert g2.cfl_limit() == dt
+        g2.step_unchecked(dt)
+    accepted = [g2.state_component_to_host(c) for c in M.COMPONENTS]
+    del g2
+    r = ref.solver(n, n, order, bc=M.PERIODIC)
+    shape = (n + 6, n + 6)
+    tol = ref.solenoidal_tolerance()
+    r.seed([a.reshape(shape) for a in rejected])
+    rel_rejected = ref.divb_relative(r, True)
+    r.seed([a.reshape(shape) for a in accepted])
+    rel_accepted = ref.divb_relative(r, True)
+    print(f"preflight trip: {len(dts)} steps, t = {sum(dts):.6g}, reference measure "
+          f"{rel_rejected:.3e} (rejected) / {rel_accepted:.3e} (accepted), tolerance {tol:.3e}")
+    assert rel_rejected > tol >= rel_accepted, (len(dts), rel_rejected, rel_accepted, tol)
