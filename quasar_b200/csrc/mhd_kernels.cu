@@ -745,8 +745,8 @@ __device__ __forceinline__ void finish_face(const Grid& g, const StateP& u, cons
 // buffers R[7][8] followed by delta[8][7], whose first 14 slots later hold
 // the projected face values w[2][7].  The R columns are padded to eight
 // doubles so that the L R = I check reads them as 16-byte pairs (half the
-// load instructions of scalar reads: the check went 41.6 -> 39.7 ms per
-// rotor 4096^2 MP7 step of reconstruction); the group stride of 114 doubles
+// load instructions of scalar reads: reconstruction went 39.9 -> 37.8 ms per
+// rotor 4096^2 MP7 step); the group stride of 114 doubles
 // puts the eight groups' 16-byte reads on distinct banks.  Padding the
 // stencil deltas the same way measured no faster.
 constexpr int kRecC = 0;    // canonical reference state, 8 components
