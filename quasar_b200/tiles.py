@@ -323,8 +323,15 @@ class TiledSolver:
         import torch
         kinds = {n: self.layout.kind_of(n) for n in COMPONENTS}
 
+        cache = {}
+
         def dev(a):
-            return torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=self.xdev)
+            # components of one kind share their index arrays: upload each once
+            key = id(a)
+            if key not in cache:
+                cache[key] = (a, torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64),
+                                                 device=self.xdev))
+            return cache[key][1]
         send, recv, images = {}, {}, []
         for p in range(self.layout.world):
             if p == self.rank:
