@@ -67,7 +67,9 @@ long long qmhd_solver_storage_size(const qmhd_solver* solver);
 
 /* seed_state(component, values): mhd_solver.cpp:521-541.  component is
  * "rho", "mx", "my", "mz", "energy", "bx"/"bx_face", "by"/"by_face",
- * "bz"/"bz_cell"; n must equal the storage size; values must be finite. */
+ * "bz"/"bz_cell"; n must equal the storage size; values must be finite
+ * (tested on the device after the copy; a rejected buffer leaves the live
+ * state unchanged). */
 int qmhd_solver_seed_state(qmhd_solver* solver, const char* component,
                            const double* values, size_t n);
 /* state_component_to_host(component): mhd_solver.cpp:586-606.  "bx"/"by"
