@@ -24,7 +24,9 @@ reference's own MHD path built for the CPU, on a bounded sample.
 Beside the plain line: `learned` = the same workload with the shipped
 troubled-cell indicator (quasar_b200/data/indicator_mp{5,7}.npz), its speed-up
 and the density L1 gap to the plain run after the same steps; `batched` = 256
-seeded independent MP5 instances on uneven grids stepped together;
+seeded independent MP5 instances on uneven grids stepped together, against
+the same instances stepped one after another, and (`batched.learned`) batched
+with the shipped MP5 indicator, with its density L1 gap to the plain batch;
 `batched_learned` = one batch of Orszag-Tang 8192^2 MP7 and 64 rotor/blast
 instances, plain and then learned (--no-learned / --no-batch skip them).
 """
@@ -468,7 +470,6 @@ def main():
         b.time_steps(3)
         bms, bzu = b.time_steps(kb)
         bms, bzu = dist.reduce(bms, "max"), dist.reduce(bzu, "sum")
-        del b
         seq_ms, seq_zu = sequential_instances(insts, kb)
         seq_ms, seq_zu = dist.reduce(seq_ms, "max"), dist.reduce(seq_zu, "sum")
         batched = {"workload": "256 seeded MP5 instances, sides log-uniform in [64, 512], "
@@ -485,6 +486,39 @@ def main():
                                          "its own solver's device-resident graph loop of the "
                                          "same steps, device times summed"},
                    "batch_over_sequential": (bzu / bms) / (seq_zu / seq_ms)}
+        if not a.no_learned:
+            # the same instances batched in learned mode (shipped MP5
+            # indicator), from the same initial states, with the plain
+            # batch's tuning and as many steps as it took (autotune trials,
+            # warm-up, timed), then the density L1 gap between the two runs
+            from quasar_b200 import train_indicator
+            from quasar_b200.indicator import attach_batch
+            bl = make_batch(insts, 5)
+            bl.set_tuning(ctas)
+            ind5, thr5 = train_indicator.load(order=5)
+            attach_batch(ind5, bl, thr5)
+            bl.time_steps(trials + 3)
+            lms, lzu = bl.time_steps(kb)
+            num = den = 0.0
+            for i, x in enumerate(insts):
+                shape = (x["ny"] + 2 * ics.nghost(5), x["nx"] + 2 * ics.nghost(5))
+                g = ics.nghost(5)
+                rp = b.instance(i).state_component_to_host("rho").reshape(shape)[g:-g, g:-g]
+                rl = bl.instance(i).state_component_to_host("rho").reshape(shape)[g:-g, g:-g]
+                num += float(np.abs(rl - rp).sum())
+                den += float(np.abs(rp).sum())
+            del bl
+            lms, lzu = dist.reduce(lms, "max"), dist.reduce(lzu, "sum")
+            num, den = dist.reduce(num, "sum"), dist.reduce(den, "sum")
+            batched["learned"] = {
+                "value": lzu / (lms * 1e-3), "ms_per_step": lms / kb,
+                "over_plain_batched": (lzu / lms) / (bzu / bms),
+                "over_sequential_plain": (lzu / lms) / (seq_zu / seq_ms),
+                "density_l1_vs_plain_batched": num / den,
+                "how": "shipped MP5 indicator on every instance; L1 = sum |rho_learned - "
+                       "rho_plain| / sum |rho_plain| over every interior cell after the same "
+                       "steps from the same initial states"}
+        del b
         if not a.no_learned:
             from quasar_b200 import train_indicator
             from quasar_b200.indicator import attach_batch

@@ -56,6 +56,13 @@ int qmhd_batch_time_steps(qmhd_batch* batch, int steps, double* ms, long long* z
 int qmhd_batch_autotune(qmhd_batch* batch, int* ctas_per_sm, int* trial_steps);
 int qmhd_batch_set_tuning(qmhd_batch* batch, const int* ctas_per_sm);
 
+/* One batched step with per-phase device times in ms (measurement hook, no
+ * counterpart in the reference): entries 0 .. QMHD_BATCH_PHASES - 1 are the
+ * tuned phases above, entry QMHD_BATCH_PHASES the rest (step begin and end;
+ * in learned mode also the indicator and the face lists).
+ * n >= QMHD_BATCH_PHASES + 1.  Every instance advances by one step. */
+int qmhd_batch_profile_step(qmhd_batch* batch, double* ms_by_phase, int n);
+
 #ifdef __cplusplus
 }
 #endif

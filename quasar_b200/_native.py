@@ -29,7 +29,7 @@ EXT_EXPORTS = ("qmhd_solver_time_auto_steps", "qmhd_solver_profile_step", "qmhd_
 TOTALS_DEVICE_MAX_CELLS = 67108864
 BATCH_EXPORTS = ("qmhd_batch_create", "qmhd_batch_destroy", "qmhd_batch_size", "qmhd_batch_zones",
                  "qmhd_batch_instance", "qmhd_batch_advance", "qmhd_batch_time_steps",
-                 "qmhd_batch_autotune", "qmhd_batch_set_tuning")
+                 "qmhd_batch_autotune", "qmhd_batch_set_tuning", "qmhd_batch_profile_step")
 INDICATOR_EXPORTS = ("qmhd_indicator_create", "qmhd_indicator_destroy", "qmhd_indicator_get_params",
                      "qmhd_indicator_set_params", "qmhd_indicator_forward",
                      "qmhd_indicator_gradient", "qmhd_indicator_collect", "qmhd_indicator_rows",
@@ -111,6 +111,7 @@ def lib() -> ctypes.CDLL:
     L.qmhd_batch_time_steps.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(ctypes.c_longlong)]
     L.qmhd_batch_autotune.argtypes = [vp, ip, ip]
     L.qmhd_batch_set_tuning.argtypes = [vp, ip]
+    L.qmhd_batch_profile_step.argtypes = [vp, dp, ctypes.c_int]
     L.qmhd_indicator_create.argtypes = [ctypes.c_ulonglong, ctypes.POINTER(vp)]
     L.qmhd_indicator_destroy.argtypes = [vp]
     L.qmhd_indicator_destroy.restype = None

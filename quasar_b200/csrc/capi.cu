@@ -338,6 +338,17 @@ int qmhd_batch_autotune(qmhd_batch* batch, int* ctas_per_sm, int* trial_steps) {
   });
 }
 
+int qmhd_batch_profile_step(qmhd_batch* batch, double* ms_by_phase, int n) {
+  return guarded([&] {
+    need(batch);
+    need(ms_by_phase);
+    if (n < QMHD_BATCH_PHASES + 1)
+      throw std::invalid_argument("qmhd_batch_profile_step: n must be >= QMHD_BATCH_PHASES + 1");
+    const std::vector<double> per = batch->impl->profile_step();
+    for (int ph = 0; ph <= QMHD_BATCH_PHASES; ++ph) ms_by_phase[ph] = per[size_t(ph)];
+  });
+}
+
 int qmhd_batch_set_tuning(qmhd_batch* batch, const int* ctas_per_sm) {
   return guarded([&] {
     need(batch);

@@ -518,7 +518,8 @@ struct InfSmem {
   static constexpr int kA1 = 128 * kHidden * 2;
   static constexpr int kPrim = kHaloX * kHaloY * 8 * 4;
   static constexpr int kOk = 256;
-  static constexpr int kTotal = kX + kW1 + kW2 + kA1 + kPrim + kOk + 64;
+  static constexpr int kVec = (3 * kHidden + 4) * 4;  // b1, b2, w3 (+ pad)
+  static constexpr int kTotal = kX + kW1 + kW2 + kA1 + kPrim + kOk + kVec + 64;
 };
 
 // One 16 x 8 block of padded cells per tile: primitives of its 20 x 12 halo
@@ -574,7 +575,11 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
   uint8_t* a1s = w2s + InfSmem::kW2;
   float* prim = reinterpret_cast<float*>(a1s + InfSmem::kA1);  // [12][20][8]
   unsigned char* okt = reinterpret_cast<unsigned char*>(prim + kHaloX * kHaloY * 8);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(okt + InfSmem::kOk);
+  // the bias and head vectors, which every thread reads at the same index
+  float* vb1 = reinterpret_cast<float*>(okt + InfSmem::kOk);
+  float* vb2 = vb1 + kHidden;
+  float* vw3 = vb2 + kHidden;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(okt + InfSmem::kOk + InfSmem::kVec);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, row = warp * 32 + lane;
   const int tx = row % kTileX, ty = row / kTileX;
@@ -585,6 +590,11 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
   if (warp == 0) tc::tmem_alloc(tslot, 128);
   stage_rows(w1s, p.w1, kHidden, kFeatPad, 0, kHidden, tid, kThreads);
   stage_rows(w2s, p.w2, kHidden, kHidden, 0, kHidden, tid, kThreads);
+  for (int e = tid; e < kHidden; e += kThreads) {
+    vb1[e] = p.b1[e];
+    vb2[e] = p.b2[e];
+    vw3[e] = p.w3[e];
+  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -658,8 +668,8 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
         uint32_t w[4];
 #pragma unroll
         for (int c = 0; c < 8; c += 2)
-          w[c / 2] = pack_bf16x2(gelu(z[h + c] + p.b1[c0 + h + c]),
-                                 gelu(z[h + c + 1] + p.b1[c0 + h + c + 1]));
+          w[c / 2] = pack_bf16x2(gelu(z[h + c] + vb1[c0 + h + c]),
+                                 gelu(z[h + c + 1] + vb1[c0 + h + c + 1]));
         *reinterpret_cast<uint4*>(a1s + tc::kmajor_offset(row, c0 + h, kHidden)) =
             make_uint4(w[0], w[1], w[2], w[3]);
       }
@@ -684,7 +694,7 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
       float z[16];
       tc::tmem_ld16(tc::tmem_addr(tb, warp * 32, 64 + c0), z);
 #pragma unroll
-      for (int c = 0; c < 16; ++c) acc += p.w3[c0 + c] * gelu(z[c] + p.b2[c0 + c]);
+      for (int c = 0; c < 16; ++c) acc += vw3[c0 + c] * gelu(z[c] + vb2[c0 + c]);
     }
     const int i = i0 + tx, j = j0 + ty;
     if (i < g.nx + g.ng && j < g.ny + g.ng) flag[g.idx(i, j)] = (forced || !(acc <= thr)) ? 1 : 0;

@@ -328,6 +328,30 @@ double MhdBatch2D::time_steps(int steps, long long* zone_updates) {
   return double(ms);
 }
 
+std::vector<double> MhdBatch2D::profile_step() {
+  prepare();
+  launch_batch_ctl(recs(0, 0), size(), 3, 0.0, kInfT, stream_);
+  cudaEvent_t start;
+  ck(cudaEventCreate(&start), "event");
+  ck(cudaEventRecord(start, stream_), "event record");
+  std::vector<cudaEvent_t> marks;
+  std::vector<int> phases;
+  enqueue_step(0, &marks, &phases);
+  ck(cudaStreamSynchronize(stream_), "profiled step");
+  std::vector<double> per(kBpCount + 1, 0.0);
+  cudaEvent_t prev = start;
+  for (size_t k = 0; k < marks.size(); ++k) {
+    float e = 0.f;
+    ck(cudaEventElapsedTime(&e, prev, marks[k]), "elapsed");
+    per[phases[k] >= 0 ? size_t(phases[k]) : size_t(kBpCount)] += e;
+    prev = marks[k];
+  }
+  for (cudaEvent_t e : marks) cudaEventDestroy(e);
+  cudaEventDestroy(start);
+  collect(nullptr);
+  return per;
+}
+
 int MhdBatch2D::autotune() {
   // candidates per phase: every CTAs-per-SM count up to the occupancy limit,
   // then one CTA per tile (0)

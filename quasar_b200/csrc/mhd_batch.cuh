@@ -45,6 +45,9 @@ class MhdBatch2D {
   // per phase: CTAs per SM of the persistent grid, 0 = one CTA per tile
   const std::vector<int>& tuning() const { return ctas_per_sm_; }
   void set_tuning(const std::vector<int>& ctas_per_sm);
+  // One step with per-phase device times in ms: kBpCount tuned phases, then
+  // the control kernels (and in learned mode the indicator and face lists).
+  std::vector<double> profile_step();
 
   // Learned troubled-cell mode for every instance (batched indicator, face
   // lists and two-pass reconstruction inside the batched step); nullptr

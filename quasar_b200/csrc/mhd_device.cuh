@@ -630,6 +630,27 @@ __device__ __forceinline__ double point_value(int q, const double* s) {
   for (int t = 0; t < N; ++t) w[t] = point_w<ORDER>(q, t);
   return wsum<N>(w, s);
 }
+// Point values at all Q = 3/4 Gauss nodes from the same N transverse
+// averages: point_value at each node, with the constant shortcut (the same
+// decision at every node) tested once.
+template <int ORDER>
+__device__ __forceinline__ void point_values(const double* s, double* out) {
+  constexpr int N = ORDER == 5 ? 5 : 7, Q = ORDER == 5 ? 3 : 4;
+  bool constant = true;
+#pragma unroll
+  for (int t = 0; t < N; ++t)
+    if (t != N / 2) constant = constant && (s[t] == s[N / 2]);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    double v = s[N / 2];
+    if (!constant) {
+      v = point_w<ORDER>(q, 0) * s[0];
+#pragma unroll
+      for (int t = 1; t < N; ++t) v += point_w<ORDER>(q, t) * s[t];
+    }
+    out[q] = v;
+  }
+}
 // Gauss average of Q = 3/4 point values.
 template <int ORDER>
 __device__ __forceinline__ double gauss_avg(const double* s) {

@@ -1486,15 +1486,24 @@ __global__ void __launch_bounds__(128) k_face_flux(Grid g, IfaceP in, FluxP out,
 
 // ---------------------------------------------------------------------------
 // MP5/MP7 face flux with one lane per Gauss point: a group of Q lanes owns a
-// face (Q = 3 at MP5, 4 at MP7).  Each lane recovers its point state and
-// solves its Riemann problem; the group votes on admissibility, gathers the
-// point fluxes in node order for the Gauss sum, and splits the stores.  Same
-// arithmetic as k_face_flux (node order of every sum kept).  The interface
-// states of a face tile (8 x 4 at MP7, 8 x 5 at MP5) and its transverse halo
-// are staged in shared memory, so each stencil row is read from L2 once per
-// tile instead of once per face row (2.8x fewer for x faces, 4x for y faces
-// at MP7).  128 threads (smaller blocks than 16 x 4 measured 3-5% faster at
-// MP7: a block waiting at the staging barrier holds fewer warps).
+// face (Q = 3 at MP5, 4 at MP7).  The interface states of a face tile (8 x 4
+// at MP7, 8 x 5 at MP5) and its transverse halo are staged in shared memory,
+// so each stencil row is read from L2 once per tile instead of once per face
+// row (2.8x fewer for x faces, 4x for y faces at MP7).  At MP7 the
+// transverse recovery is split by component: lane q forms components q,
+// q + 4, ... at every Gauss point of its face (each stencil column read
+// once, and the constant-stencil shortcut, which decides the same for every
+// point, tested once per component) into the face's point rows in shared
+// memory, from which each lane takes its own point's 16 components as
+// 16-byte pairs.  Each lane solves its point's Riemann problem, the group
+// votes on admissibility, and the point fluxes go back through the same
+// rows, where lane q forms and stores the Gauss sums of components q, q + 4
+// (rotor 4096^2 MP7: face flux 27.6 -> 23.3 ms per step; Orszag-Tang 2048^2
+// MP7: 10.8 -> 10.4).  At MP5 each lane recovers its own point (below).
+// Same sums in the same node order as k_face_flux; the compiler's fused
+// multiply-adds may pair differently, a rounding-level difference.  128 threads
+// (smaller blocks than 16 x 4 measured 3-5% faster at MP7: a block waiting
+// at the staging barrier holds fewer warps).
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1507,14 +1516,25 @@ template <int ORDER>
 constexpr int fq_ty() { return ORDER == 5 ? 5 : 4; }
 // 96 registers (ptxas keeps a few values of the HLLD tail on the stack):
 // five 128-thread blocks per SM measured 8-11% faster than four at 128
-// registers (six spill more and lose it again).  Staging the tile
-// face-major so that lanes read component pairs as 16-byte loads measured
-// 9% slower (more spills at this register cap).
+// registers (six spill more and lose it again).
 constexpr int kFqBlocksPerSm = 5;
+// Shared-memory strides in doubles.  A component plane of the tile is padded
+// to 4 mod 16 doubles, so that the lanes of a group (components 4 apart of
+// one cell) and the neighbouring groups (neighbouring cells) read distinct
+// banks; a point row is 16 components + 2 (16-byte aligned), a face's rows
+// are Q rows + 4.
+constexpr int fq_plane(int cells) { return cells + ((4 - cells % 16) + 16) % 16; }
+constexpr int kFqRow = 18;
+template <int ORDER>
+constexpr int fq_face() { return (ORDER == 5 ? 3 : 4) * kFqRow + 4; }
 
-// TX: faces per tile row; the block is four warps of 32 / Q groups each.
+// Per-point recovery (MP5): each lane forms all 16 components of its own
+// Gauss point from the staged tile, and the group gathers the point fluxes
+// by shuffles.  With three lanes per face the component split below leaves
+// a lane with six components against five and measured 8% slower on
+// Orszag-Tang 2048^2 MP5 (face flux 9.1 -> 9.8 ms per step).
 template <int DIR, int ORDER, int TX = kFqTX>
-__device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, const FluxP& out,
+__device__ __forceinline__ void b_face_flux_pt(const Grid& g, const IfaceP& in, const FluxP& out,
                                                double* emf, int* nj, double* spd, double gamma,
                                                const Ctl* ctl, int bx, int by) {
   constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
@@ -1672,6 +1692,200 @@ __device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, 
   }
   const unsigned nproof = (__ballot_sync(gmask, proof == 0) >> base) & ((1u << Q) - 1u);
   if (lane == 0) nj[k] = nproof == 0 ? 1 : 0;
+}
+
+// Component-split recovery (MP7), as described above.
+template <int DIR, int ORDER, int TX = kFqTX>
+__device__ __forceinline__ void b_face_flux_cs(const Grid& g, const IfaceP& in, const FluxP& out,
+                                               double* emf, int* nj, double* spd, double gamma,
+                                               const Ctl* ctl, int bx, int by) {
+  constexpr int H = ORDER == 5 ? 2 : 3, N = 2 * H + 1, Q = ORDER == 5 ? 3 : 4;
+  constexpr int FPW = 32 / Q, TY = fq_ty<ORDER>();         // faces per warp, tile rows
+  static_assert(4 * FPW == TX * TY, "four warps cover the face tile");
+  constexpr int TR = DIR == 0 ? TY + 2 * H : TY;          // tile rows (j)
+  constexpr int TC = DIR == 0 ? TX : TX + 2 * H;          // tile columns (i)
+  constexpr int PS = fq_plane(TR * TC), FS = fq_face<ORDER>();
+  __shared__ double tile[16 * PS];             // component c of slot (row, col): c PS + row TC + col
+  __shared__ unsigned char same[TR][TC];       // staged and L == R in every component
+  __shared__ __align__(16) double pts[4 * FPW * FS];  // per face: Q point rows
+  if (ctl->status) return;  // uniform over the block
+  const int i0 = bx * TX, j0 = by * TY;
+  const bool perx = g.bc[0] == 0 && g.bc[1] == 0, pery = g.bc[2] == 0 && g.bc[3] == 0;
+  for (int e = threadIdx.x; e < TR * TC; e += blockDim.x) {
+    const int row = e / TC, col = e - row * TC;
+    int fi, fj;
+    bool valid;
+    if (DIR == 0) {
+      const int ii = i0 + col;
+      fi = (ii == g.nx && perx) ? 0 : ii;
+      fj = j0 - H + row;
+      valid = ii <= g.nx && fj >= -g.ng && fj < g.ny + g.ng;
+    } else {
+      const int jj = j0 + row;
+      fj = (jj == g.ny && pery) ? 0 : jj;
+      fi = i0 - H + col;
+      valid = jj <= g.ny && fi >= -g.ng && fi < g.nx + g.ng;
+    }
+    const long long kk = valid ? g.idx(fi, fj) : 0;
+    bool eq = valid;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double a = valid ? __ldg(in.L[c] + kk) : 0.0;
+      const double b = valid ? __ldg(in.R[c] + kk) : 0.0;
+      tile[c * PS + e] = a;
+      tile[(8 + c) * PS + e] = b;
+      eq = eq && a == b;
+    }
+    same[row][col] = eq;
+  }
+  __syncthreads();
+  constexpr bool kLF = false;
+  const int wl = threadIdx.x & 31;
+  if (wl >= FPW * Q) return;  // the lanes no group uses (MP5)
+  const int lane = wl % Q, base = wl - lane;
+  const unsigned gmask = ((1u << Q) - 1u) << base;
+  const int face = (threadIdx.x >> 5) * FPW + wl / Q;
+  const int fx = face % TX, fy = face / TX;
+  const int i = i0 + fx, j = j0 + fy;
+  if (i > g.nx || j > g.ny) return;  // whole groups leave together
+  const long long k = g.idx(i, j);
+  const double h = DIR == 0 ? g.dx : g.dy;
+  // tile slot of stencil tap t (t = H is the face itself)
+  auto slot = [&](int t) { return DIR == 0 ? (fy + t) * TC + fx : fy * TC + fx + t; };
+  double* const fp = pts + face * FS;  // this face's point rows
+  // point values of components lane, lane + Q, ... at the Q Gauss nodes
+#pragma unroll
+  for (int m = 0; m < (16 + Q - 1) / Q; ++m) {
+    const int c = lane + Q * m;
+    if (c < 16) {
+      double s[N], v[Q];
+#pragma unroll
+      for (int t = 0; t < N; ++t) s[t] = tile[c * PS + slot(t)];
+      point_values<ORDER>(s, v);
+#pragma unroll
+      for (int p = 0; p < Q; ++p) fp[p * kFqRow + c] = v[p];
+    }
+  }
+  __syncwarp(gmask);
+  St l, r;
+  {
+    const double2* row = reinterpret_cast<const double2*>(fp + lane * kFqRow);
+    const double2 a0 = row[0], a1 = row[1], a2 = row[2], a3 = row[3];
+    const double2 b0 = row[4], b1 = row[5], b2 = row[6], b3 = row[7];
+    l = St{a0.x, a0.y, a1.x, a1.y, a2.x, a2.y, a3.x, a3.y};
+    r = St{b0.x, b0.y, b1.x, b1.y, b2.x, b2.y, b3.x, b3.y};
+  }
+  double irl = 1.0 / l.rho, irr = 1.0 / r.rho;
+  const bool ok = point_admissible_ir(l, gamma, irl) && point_admissible_ir(r, gamma, irr);
+  auto centre = [&](bool left) {
+    const int o = left ? 0 : 8, sc = slot(H);
+    return St{tile[o * PS + sc],       tile[(o + 1) * PS + sc], tile[(o + 2) * PS + sc],
+              tile[(o + 3) * PS + sc], tile[(o + 4) * PS + sc], tile[(o + 5) * PS + sc],
+              tile[(o + 6) * PS + sc], tile[(o + 7) * PS + sc]};
+  };
+  const unsigned bad = (__ballot_sync(gmask, !ok) >> base) & ((1u << Q) - 1u);
+  const bool group_ok = bad == 0;
+  const int first_bad = bad ? __ffs(bad) - 1 : Q;
+  double rate = 0.0;
+  if (spd) {
+    if (lane == 0) rate = face_rate<DIR, ORDER>(centre(true), centre(false), gamma, h);
+    if (lane < first_bad) rate = fmax(rate, face_rate<DIR, ORDER>(l, r, gamma, h));
+  }
+  const bool solve = group_ok || lane == 0;
+  if (!group_ok) {
+    l = centre(true);
+    r = centre(false);
+    irl = 1.0 / l.rho;
+    irr = 1.0 / r.rho;
+  }
+  double fv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (solve) {
+    const Fx f = riemann<DIR>(l, r, kLF, gamma, irl, irr);
+    fv[0] = f.rho; fv[1] = f.mx; fv[2] = f.my; fv[3] = f.mz;
+    fv[4] = f.E;   fv[5] = f.bx; fv[6] = f.by; fv[7] = f.bz;
+  }
+  // the point fluxes replace the lane's own point row (no other lane reads
+  // it after the exchange above)
+  {
+    double2* row = reinterpret_cast<double2*>(fp + lane * kFqRow);
+    row[0] = make_double2(fv[0], fv[1]);
+    row[1] = make_double2(fv[2], fv[3]);
+    row[2] = make_double2(fv[4], fv[5]);
+    row[3] = make_double2(fv[6], fv[7]);
+  }
+  __syncwarp(gmask);
+  // Gauss sums of components lane, lane + Q, ... in node order (or lane 0's
+  // single solve at the face state when a point was not admissible)
+  constexpr int RC = (8 + Q - 1) / Q;
+  double res[RC];
+#pragma unroll
+  for (int m = 0; m < RC; ++m) {
+    const int c = lane + Q * m;
+    res[m] = 0.0;
+    if (c < 8) {
+      if (group_ok) {
+        double sq[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) sq[q] = fp[q * kFqRow + c];
+        res[m] = gauss_avg<ORDER>(sq);
+      } else {
+        res[m] = fp[c];
+      }
+    }
+  }
+  // out, emf and nj may each be absent (the per-kernel launch interface
+  // asks for fluxes or for the CT face tables alone)
+  if (out.f[0]) {
+#pragma unroll
+    for (int m = 0; m < RC; ++m)
+      if (lane + Q * m < 8) out.f[lane + Q * m][k] = res[m];
+  }
+  // face E_z = -F(by) of an x face, F(bx) of a y face: the lane holding it
+  constexpr int EC = DIR == 0 ? 6 : 5;
+  if (emf && lane == EC % Q) emf[k] = DIR == 0 ? -res[EC / Q] : res[EC / Q];
+  if (spd) {
+    double m = rate;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) m = fmax(m, __shfl_sync(gmask, rate, base + q));
+    if (lane == 0) spd[k] = m;
+  }
+  if (!nj) return;  // uniform over the block
+  // no-jump proof over the 2H+1 transverse taps (mapped like every CT table
+  // read), split across the group.  A tap whose mapped face is the one staged
+  // in its tile slot reads the staged comparison; the others read memory.
+  int proof = 1;
+  for (int off = lane - H; off <= H; off += Q) {
+    const int mi = face_index(DIR == 0 ? i : i + off, g.nx, g.bc[0], g.bc[1]);
+    const int mj = face_index(DIR == 0 ? j + off : j, g.ny, g.bc[2], g.bc[3]);
+    const int ti = DIR == 0 ? ((i == g.nx && perx) ? 0 : i) : i + off;
+    const int tj = DIR == 0 ? j + off : ((j == g.ny && pery) ? 0 : j);
+    if (mi == ti && mj == tj) {
+      const int sl = slot(off + H);
+      if (!same[sl / TC][sl % TC]) proof = 0;
+      continue;
+    }
+    if (!in_pad(g, mi, mj)) {
+      proof = 0;
+      break;
+    }
+    const long long km = g.idx(mi, mj);
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (!(in.L[c][km] == in.R[c][km])) proof = 0;
+  }
+  const unsigned nproof = (__ballot_sync(gmask, proof == 0) >> base) & ((1u << Q) - 1u);
+  if (lane == 0) nj[k] = nproof == 0 ? 1 : 0;
+}
+
+// TX: faces per tile row; the block is four warps of 32 / Q groups each.
+template <int DIR, int ORDER, int TX = kFqTX>
+__device__ __forceinline__ void b_face_flux_qs(const Grid& g, const IfaceP& in, const FluxP& out,
+                                               double* emf, int* nj, double* spd, double gamma,
+                                               const Ctl* ctl, int bx, int by) {
+  if constexpr (ORDER == 7)
+    b_face_flux_cs<DIR, ORDER, TX>(g, in, out, emf, nj, spd, gamma, ctl, bx, by);
+  else
+    b_face_flux_pt<DIR, ORDER, TX>(g, in, out, emf, nj, spd, gamma, ctl, bx, by);
 }
 
 template <int DIR, int ORDER>
@@ -1933,8 +2147,16 @@ __device__ __forceinline__ void b_cell_emf_s(const Grid& g, const StateP& u, dou
         double smp[N];
 #pragma unroll
         for (int t = 0; t < N; ++t) smp[t] = X[(c * SY + threadIdx.y + t) * TX + threadIdx.x];
+        if constexpr (ORDER == 7) {
+          // the constant-stencil test once for the four y-nodes
+          double pv[Q];
+          point_values<ORDER>(smp, pv);
 #pragma unroll
-        for (int qy = 0; qy < Q; ++qy) st[qy][c] = point_value<ORDER>(qy, smp);
+          for (int qy = 0; qy < Q; ++qy) st[qy][c] = pv[qy];
+        } else {
+#pragma unroll
+          for (int qy = 0; qy < Q; ++qy) st[qy][c] = point_value<ORDER>(qy, smp);
+        }
       }
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) {
@@ -2494,11 +2716,38 @@ template <int DIR, int ORDER>
 __global__ void __launch_bounds__(128, 4) kb_reconstruct_list(const BatchRec* __restrict__ r,
                                                               const BatchLearnRec* __restrict__ l,
                                                               int n) {
-  for (int inst = 0; inst < n; ++inst) {
+  // Work units are the 32-entry chunks of every instance's list, numbered
+  // across the instances in order; warp w of the grid takes chunks w, w + W,
+  // ... and walks the instances' chunk counts (device values, warp-uniform)
+  // alongside, so that many small lists run side by side instead of one
+  // list at a time.  A chunk is the same 32 entries the single-instance
+  // list pass gives a warp.
+  extern __shared__ double dsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* ws = dsm + warp * kWarpReconDoubles;
+  const long long stride = (long long)gridDim.x * kReconWarps;
+  long long c = (long long)blockIdx.x * kReconWarps + warp;  // this warp's next chunk
+  long long first = 0;  // number of the first chunk of instance `inst`
+  for (int inst = 0; inst < n;) {
     const BatchRec& q = r[inst];
-    if (q.a.ctl->status & ~kStatusDone) continue;
-    b_reconstruct_list<DIR, ORDER>(q.a.g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma,
-                                   DIR == 0 ? l[inst].xlist : l[inst].ylist, l[inst].counts[DIR]);
+    const int cnt = (q.a.ctl->status & ~kStatusDone) ? 0 : l[inst].counts[DIR];
+    const long long chunks = (cnt + 31) / 32;
+    if (c >= first + chunks) {
+      first += chunks;
+      ++inst;
+      continue;
+    }
+    const int t = int(c - first) * 32 + lane;
+    const bool valid = t < cnt;
+    const Grid& g = q.a.g;
+    int i = 0, j = 0;
+    if (valid) {
+      const int k = (DIR == 0 ? l[inst].xlist : l[inst].ylist)[t];
+      i = k % g.pitch - g.ng;
+      j = k / g.pitch - g.ng;
+    }
+    mp_faces_warp<DIR, ORDER>(g, q.a.u, DIR == 0 ? q.a.ix : q.a.iy, q.a.gamma, i, j, valid, ws);
+    c += stride;
   }
 }
 

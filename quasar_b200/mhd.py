@@ -358,6 +358,14 @@ class MhdBatch2D:
         _native.check(_native.lib().qmhd_batch_autotune(self._h, c, ctypes.byref(t)))
         return list(c), t.value
 
+    def profile_step(self) -> dict:
+        """One step of every instance with per-phase device times (ms)."""
+        ms = (ctypes.c_double * (self.PHASES + 1))()
+        _native.check(_native.lib().qmhd_batch_profile_step(self._h, ms, self.PHASES + 1))
+        names = ["recon_x", "recon_y", "face_flux", "cell_emf", "corner_emf", "update",
+                 "collocation", "ghosts_x", "ghosts_y", "control"]
+        return dict(zip(names, ms[:]))
+
     def set_tuning(self, ctas_per_sm) -> None:
         c = (ctypes.c_int * self.PHASES)(*[int(x) for x in ctas_per_sm])
         _native.check(_native.lib().qmhd_batch_set_tuning(self._h, c))
