@@ -201,9 +201,9 @@ void MhdBatch2D::enqueue_step(int par, std::vector<cudaEvent_t>* marks,
     const BatchRec* r = recs(par, st);
     const bool first = st == 0;
     if (ind_) {
-      launch_batch_reconstruct_learned(r, learn_, plan_[kBpRecon0], 0, order_, 2 * sms_, stream_);
+      launch_batch_reconstruct_learned(r, learn_, plan_[kBpRecon0], 0, order_, 4 * sms_, stream_);
       mark(kBpRecon0);
-      launch_batch_reconstruct_learned(r, learn_, plan_[kBpRecon1], 1, order_, 2 * sms_, stream_);
+      launch_batch_reconstruct_learned(r, learn_, plan_[kBpRecon1], 1, order_, 4 * sms_, stream_);
       mark(kBpRecon1);
     } else {
       launch_batch_reconstruct(r, plan_[kBpRecon0], 0, order_, stream_);

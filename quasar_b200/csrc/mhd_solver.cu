@@ -365,8 +365,8 @@ void MhdSolver2D::reconstruct_stage(const StageArgs& a, int order) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    launch_reconstruct_learned(a, 0, flags_, flists_, fcounts_, 2 * sms, stream_);
-    launch_reconstruct_learned(a, 1, flags_, flists_ + g_.size(), fcounts_ + 1, 2 * sms, stream_);
+    launch_reconstruct_learned(a, 0, flags_, flists_, fcounts_, 4 * sms, stream_);
+    launch_reconstruct_learned(a, 1, flags_, flists_ + g_.size(), fcounts_ + 1, 4 * sms, stream_);
   } else {
     launch_reconstruct(a, 0, stream_);
     launch_reconstruct(a, 1, stream_);
