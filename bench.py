@@ -500,6 +500,7 @@ def main():
             bl.time_steps(trials + 3)
             lms, lzu = bl.time_steps(kb)
             num = den = 0.0
+            dvb = {"max": 0.0, "rel": 0.0, "max_plain": 0.0, "rel_plain": 0.0}
             for i, x in enumerate(insts):
                 shape = (x["ny"] + 2 * ics.nghost(5), x["nx"] + 2 * ics.nghost(5))
                 g = ics.nghost(5)
@@ -507,14 +508,21 @@ def main():
                 rl = bl.instance(i).state_component_to_host("rho").reshape(shape)[g:-g, g:-g]
                 num += float(np.abs(rl - rp).sum())
                 den += float(np.abs(rp).sum())
+                for key, s_ in (("", bl.instance(i)), ("_plain", b.instance(i))):
+                    dvb["max" + key] = max(dvb["max" + key], s_.divergence_b_max())
+                    dvb["rel" + key] = max(dvb["rel" + key], s_.divergence_b_relative())
             del bl
             lms, lzu = dist.reduce(lms, "max"), dist.reduce(lzu, "sum")
             num, den = dist.reduce(num, "sum"), dist.reduce(den, "sum")
+            dvb = {k: dist.reduce(v, "max") for k, v in dvb.items()}
             batched["learned"] = {
                 "value": lzu / (lms * 1e-3), "ms_per_step": lms / kb,
                 "over_plain_batched": (lzu / lms) / (bzu / bms),
                 "over_sequential_plain": (lzu / lms) / (seq_zu / seq_ms),
                 "density_l1_vs_plain_batched": num / den,
+                "div_b": dict(dvb, note="max over instances of max|div B| and of the reference's "
+                                        "relative measure max|div B| dx / max|B_face|, learned "
+                                        "and plain batch after the same steps"),
                 "how": "shipped MP5 indicator on every instance; L1 = sum |rho_learned - "
                        "rho_plain| / sum |rho_plain| over every interior cell after the same "
                        "steps from the same initial states"}
