@@ -93,6 +93,27 @@ def test_autotuned_batch_still_equals_instances():
     assert ms > 0 and zu == 2 * b.zones()
 
 
+def test_profiled_batch_step_is_a_batched_step():
+    """qmhd_batch_profile_step: one step of every instance (the same state as
+    stepping each alone) with a non-negative device time per phase."""
+    order = 7
+    insts = mixed_instances(order, count=3, seed=14)
+    b = mhd.MhdBatch2D([config(x, order) for x in insts])
+    alone = [mhd.MhdSolver2D(config(x, order)) for x in insts]
+    for i, x in enumerate(insts):
+        for name, a in zip(ics.COMPONENTS, x["arrays"]()):
+            b.instance(i).seed_state(name, a)
+            alone[i].seed_state(name, a)
+    ph = b.profile_step()
+    assert len(ph) == mhd.MhdBatch2D.PHASES + 1
+    assert all(np.isfinite(v) and v >= 0.0 for v in ph.values()) and sum(ph.values()) > 0.0
+    for i, x in enumerate(insts):
+        _, k = alone[i].advance_auto(0.0, 1e30, 1)
+        assert k == 1
+        err = rounding_gap(read_all(b.instance(i), x, order), read_all(alone[i], x, order))
+        assert err <= BATCH_TOL, (x["family"], i, err)
+
+
 def test_batch_rejects_mixed_orders():
     insts = mixed_instances(5, count=2)
     with pytest.raises(ValueError):
