@@ -196,6 +196,26 @@ __device__ __forceinline__ Norm make_norm(const float* c, double gamma) {
 __device__ __forceinline__ float clampf(float x) {
   return isfinite(x) ? fminf(fmaxf(x, -64.0f), 64.0f) : 64.0f;
 }
+// The same from the two 16-byte halves of the stencil cell (rho, vx, vy, vz)
+// and (p, bx, by, bz) and of the centre c.
+__device__ __forceinline__ uint4 features8h(const float4 qa, const float4 qb, const float4 ca,
+                                            const float4 cb, const Norm& n) {
+  float f[8];
+  f[0] = clampf(qa.x * n.irho - 1.0f);
+  f[1] = clampf((qa.y - ca.y) * n.ia);
+  f[2] = clampf((qa.z - ca.z) * n.ia);
+  f[3] = clampf((qa.w - ca.w) * n.ia);
+  f[4] = clampf(qb.x * n.ip - 1.0f);
+  f[5] = clampf((qb.y - cb.y) * n.isb);
+  f[6] = clampf((qb.z - cb.z) * n.isb);
+  f[7] = clampf((qb.w - cb.w) * n.isb);
+  uint4 r;
+  r.x = pack_bf16x2(f[0], f[1]);
+  r.y = pack_bf16x2(f[2], f[3]);
+  r.z = pack_bf16x2(f[4], f[5]);
+  r.w = pack_bf16x2(f[6], f[7]);
+  return r;
+}
 // 8 normalised features of stencil cell q (primitives) as packed BF16.
 __device__ __forceinline__ uint4 features8(const float* q, const float* c, const Norm& n) {
   float f[8];
@@ -573,7 +593,13 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
   uint8_t* w1s = xs + InfSmem::kX;
   uint8_t* w2s = w1s + InfSmem::kW1;
   uint8_t* a1s = w2s + InfSmem::kW2;
-  float* prim = reinterpret_cast<float*>(a1s + InfSmem::kA1);  // [12][20][8]
+  // halo primitives in two planes of 16-byte records, (rho, vx, vy, vz) and
+  // (p, bx, by, bz) per cell, so that eight lanes reading eight neighbouring
+  // cells read 128 contiguous bytes (one 32-byte record per cell put two
+  // lanes on the same banks)
+  float* prim = reinterpret_cast<float*>(a1s + InfSmem::kA1);
+  float4* pra = reinterpret_cast<float4*>(prim);            // [12][20]
+  float4* prb = pra + kHaloX * kHaloY;                       // [12][20]
   unsigned char* okt = reinterpret_cast<unsigned char*>(prim + kHaloX * kHaloY * 8);
   // the bias and head vectors, which every thread reads at the same index
   float* vb1 = reinterpret_cast<float*>(okt + InfSmem::kOk);
@@ -619,8 +645,8 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
       float w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       if (ci >= -g.ng && ci < g.nx + g.ng && cj >= -g.ng && cj < g.ny + g.ng)
         good = cell_prim(u, g.idx(ci, cj), gamma, w);
-#pragma unroll
-      for (int q = 0; q < 8; ++q) prim[e * 8 + q] = w[q];
+      pra[e] = make_float4(w[0], w[1], w[2], w[3]);
+      prb[e] = make_float4(w[4], w[5], w[6], w[7]);
       okt[e] = good ? 1 : 0;
     }
     __syncthreads();
@@ -629,13 +655,17 @@ __global__ void __launch_bounds__(kThreads) k_indicator(Src src, MlpDev p, float
       bool all = true;
       for (int dj = 0; dj < 5; ++dj)
         for (int di = 0; di < 5; ++di) all = all && okt[(ty + dj) * kHaloX + tx + di] != 0;
-      const float* c = prim + ((ty + 2) * kHaloX + tx + 2) * 8;
+      const int ce = (ty + 2) * kHaloX + tx + 2;
+      const float4 ca = pra[ce], cb = prb[ce];
       if (all) {
+        const float c[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
         const Norm nm = make_norm(c, gamma);
         for (int dj = 0; dj < 5; ++dj)
-          for (int di = 0; di < 5; ++di)
+          for (int di = 0; di < 5; ++di) {
+            const int q = (ty + dj) * kHaloX + tx + di;
             *reinterpret_cast<uint4*>(xs + tc::kmajor_offset(row, 8 * (5 * dj + di), kFeatPad)) =
-                features8(prim + ((ty + dj) * kHaloX + tx + di) * 8, c, nm);
+                features8h(pra[q], prb[q], ca, cb, nm);
+          }
       } else {
         forced = true;
         for (int q = 0; q < 25; ++q)
